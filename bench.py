@@ -1,0 +1,362 @@
+"""Benchmark: voxel-view updates/s of the tilt WBP hot path on B200.
+
+Workload (one "step" = one pass of the hot path over one tilt series, inputs
+resident in HBM): large plain WBP, 121 views at -60..+60 deg in 1 deg steps
+with N(0, 0.1 deg) jitter, 2048x2048 float32 projections of a seeded phantom
+(5000 ellipsoids + 200 beads, Poisson-like noise), reconstructed to
+2048 x 2048 x 800 (13.4 GB resident).  The pass is R-weighting + cosine stretch
+(filter stage) and back-projection.  It runs in two forms: FP16-stored
+filtered projections (the headline `value`) and plain FP32 (`plain_fp32`);
+both accumulate in FP32.  Inputs (2 GB projections, 2-4 GB staged rows, 13.4 GB
+volume) are far larger than L2, so no flush is needed between steps.
+
+`e2e` goes through the public C ABI with pinned host buffers: upload the
+projections, reconstruct, download the whole volume, every step.
+
+--impl reference: the CPU restatement of the reference's own algorithm (the
+Rust reference cannot be built here) on a bounded sample of the same workload,
+all host threads.
+
+Multi-GPU (torchrun): one independent series per rank (weak scaling), no
+data-path collective; the time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "imod-rs_b200"))
+
+METRIC = "voxel-view updates/s"
+SM_COUNT = 148
+SMEM_BYTES_PER_CLK = 128  # per SM
+
+
+def c2_workload(jitter_seed=2):
+    rng = np.random.default_rng(jitter_seed)
+    ang = (np.arange(-60, 61, 1.0) + rng.normal(0.0, 0.1, 121)).astype(np.float32)
+    return dict(nx=2048, ny=2048, onx=2048, onz=800, angles=ang, radial=(0.35, 0.035))
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local, dist
+
+
+def max_over_ranks(x, dist, world):
+    if world <= 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, dist, world):
+    if world <= 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(dist, world):
+    if world > 1:
+        dist.barrier()
+
+
+def read_traffic():
+    """Per-launch DRAM traffic of the back-projection kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "bp_fast_c2_fp16.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+def run_ours(args):
+    import torch
+
+    import tiltgpu as T
+
+    world, rank, local, dist = dist_setup(args)
+    torch.cuda.set_device(local)
+    w = c2_workload()
+    nx, ny, onx, onz, ang = w["nx"], w["ny"], w["onx"], w["onz"], w["angles"]
+    nz = len(ang)
+    n_proj = nz * ny * nx
+    # seeded phantom projections, generated on this rank's device (independent series per rank)
+    proj_d = torch.empty(n_proj, dtype=torch.float32, device=f"cuda:{local}")
+    T.synth_projections(ang, nx=nx, ny=ny, vol_nx=onx, vol_nz=onz, n_ell=5000, rmin=3, rmax=40,
+                        dmin=0.2, dmax=1.0, n_beads=200, bead_r=5, bead_d=5.0, noise_kind=2,
+                        noise=20000.0, seed=1000 + rank, device=local, out_device_ptr=proj_d.data_ptr())
+    stream = torch.cuda.current_stream()
+    results = {}
+    launches = 0
+    for form in ("fp32", "fp16"):
+        s = T.Session(nx, ny, nz, ang, width=onx, thickness=onz, radial=w["radial"], log=True,
+                      storage=form, device=local)
+        s.set_stream(stream.cuda_stream)
+        s.set_device(proj_d.data_ptr(), n_proj)
+        for _ in range(args.warmup):
+            s.reconstruct(sync=False)
+        torch.cuda.synchronize()
+        barrier(dist, world)
+        clocks = ClockSampler(local)
+        if form == "fp16":
+            clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        bp_ms = []
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            s.reconstruct(sync=False)
+            info = s.last_run()
+            launches += info["kernel_launches"] if form == "fp16" else 0
+        e1.record(stream)
+        torch.cuda.synchronize()
+        # per-stage device times of the last step (events on the launching stream)
+        s.synchronize()
+        info = s.last_run()
+        barrier(dist, world)
+        ms = e0.elapsed_time(e1)
+        ms_max = max_over_ranks(ms, dist, world)
+        upd = info["updates"] * args.steps
+        results[form] = dict(ms=ms_max, updates=sum_over_ranks(upd, dist, world), info=info,
+                             kernel=s.kernel_info(),
+                             clocks=clocks.stop() if form == "fp16" else None)
+        # back-projection kernel alone, timed on the launching stream
+        bp = []
+        for _ in range(3):
+            s.reconstruct(sync=True)
+            bp.append(s.last_run()["ms_backproject"])
+        results[form]["bp_ms"] = float(np.median(bp))
+        results[form]["filter_ms"] = float(s.last_run()["ms_filter"])
+        if form == "fp16":
+            sess16 = s
+        else:
+            s.close()
+    # ---- e2e through the public API with pinned host buffers
+    s = sess16
+    host_in = torch.empty(n_proj, dtype=torch.float32, pin_memory=True)
+    host_in.copy_(proj_d.cpu())
+    out_shape = s.out_shape
+    host_out = torch.empty(int(np.prod(out_shape)), dtype=torch.float32, pin_memory=True)
+    import ctypes as C
+    L = T.lib()
+    st = T.Stats()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(1):
+        T.check(L.tg_upload_projections(s.h, C.c_void_p(host_in.data_ptr()), n_proj))
+        T.check(L.tg_reconstruct(s.h))
+        T.check(L.tg_download_slices(s.h, 0, out_shape[0], C.c_void_p(host_out.data_ptr()), C.byref(st)))
+    torch.cuda.synchronize()
+    barrier(dist, world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):  # H2D, reconstruct and D2H all run on `stream`
+        T.check(L.tg_upload_projections(s.h, C.c_void_p(host_in.data_ptr()), n_proj))
+        T.check(L.tg_reconstruct(s.h))
+        T.check(L.tg_download_slices(s.h, 0, out_shape[0], C.c_void_p(host_out.data_ptr()), C.byref(st)))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(e0.elapsed_time(e1) * 1e-3, dist, world)
+    e2e_upd = sum_over_ranks(s.last_run()["updates"] * e2e_steps, dist, world)
+    s.close()
+    del host_in, host_out
+
+    r16, r32 = results["fp16"], results["fp32"]
+    value = r16["updates"] / (r16["ms"] * 1e-3)
+    plain = r32["updates"] / (r32["ms"] * 1e-3)
+    clk = r16["clocks"] or {}
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    # roofline of the dominant kernel (back-projection): shared-memory bytes per update
+    # (4 B FP16 pair, 8 B FP32 pair) against 148 SMs x 128 B/clk x measured SM clock
+    upd_pass = r16["info"]["updates"]
+    bp_s = r16["bp_ms"] * 1e-3
+    ach = upd_pass * 4.0 / bp_s / 1e9
+    peak = SM_COUNT * SMEM_BYTES_PER_CLK * sm_mhz * 1e6 / 1e9
+    traffic = read_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r16["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "storage": "fp16",
+        "data": "synthetic (seeded ellipsoid+bead phantom, Poisson noise, --log)",
+        "config": {"workload": "large plain WBP: 121 views 2048x2048 -> 2048x2048x800, RADIAL 0.35/0.035",
+                   "views": nz, "proj": [nx, ny], "volume": [onx, ny, onz],
+                   "l2": "inputs larger than L2 (no flush needed)", "parallelism": f"replicas{world}",
+                   "bp_kernel": r16["kernel"]["variant_name"]},
+        "plain_fp32": {"value": plain, "ms_per_step": r32["ms"] / args.steps,
+                       "bp_ms": r32["bp_ms"], "filter_ms": r32["filter_ms"],
+                       "bp_kernel": r32["kernel"]["variant_name"],
+                       "roofline_frac": upd_pass * 8.0 / (r32["bp_ms"] * 1e-3) / 1e9 / peak},
+        "fp16_over_fp32": value / plain,
+        "stage_ms": {"filter": r16["filter_ms"], "backproject": r16["bp_ms"]},
+        "roofline": {"bound": "smem", "achieved": ach, "peak": peak, "unit": "GB/s",
+                     "frac": ach / peak, "traffic": traffic,
+                     "note": "shared-memory bytes of the back-projection kernel (4 B/update FP16 pair); "
+                             "peak = 148 SMs x 128 B/clk x median SM clock sampled in the run"},
+        "roofline_hbm": {"bound": "hbm", "achieved": (4.0 * nz * nx * ny + 4.0 * onx * onz * ny) / bp_s / 1e9,
+                         "peak": 6548.2, "unit": "GB/s", "note": "of measured (MEASURED_PEAKS.json)"},
+        "e2e": {"value": e2e_upd / e2e_s, "unit": "updates/s", "h2d_bytes_per_step": n_proj * 4,
+                "d2h_bytes_per_step": int(np.prod(out_shape)) * 4 + 12},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, w, proj_d)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(args, w, proj_d=None, nslices=16):
+    """The oracle port (ref32, all host threads) on slices [0, nslices) of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    nx, ny, onx, onz, ang = w["nx"], w["ny"], w["onx"], w["onz"], w["angles"]
+    nz = len(ang)
+    if proj_d is not None:
+        proj = proj_d.cpu().numpy().reshape(nz, ny, nx)
+    else:
+        proj = seeded_rows(nz, ny, nx, nslices)
+    p = O.Params(nx, ny, nz, ang, width=onx, thickness=onz, radial=w["radial"], log=True)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    O.wbp_rows(p, proj, 0, nslices, nthreads=cores)
+    dt = time.perf_counter() - t0
+    upd = float(onx) * onz * nslices * nz
+    return {"value": upd / dt, "unit": "updates/s", "cores": cores, "kind": "port",
+            "sample": f"slices 0..{nslices} of the workload (filter of their rows + stretch + WBP), "
+                      f"{upd:.3g} updates in {dt:.2f} s"}
+
+
+def seeded_rows(nz, ny, nx, nrows, seed=5):
+    """Seeded Poisson-like counts for the rows a bounded CPU sample reads (timing is data-independent)."""
+    rng = np.random.default_rng(seed)
+    proj = np.full((nz, ny, nx), 20000.0, np.float32)
+    proj[:, :nrows, :] = rng.poisson(20000.0 * np.exp(-rng.random((nz, nrows, nx)))).astype(np.float32)
+    return proj
+
+
+def run_reference(args):
+    world, rank, local, dist = dist_setup(args)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    w = c2_workload()
+    nx, ny, onx, onz, ang = w["nx"], w["ny"], w["onx"], w["onz"], w["angles"]
+    nz = len(ang)
+    nsl = 8
+    proj = seeded_rows(nz, ny, nx, nsl)
+    p = O.Params(nx, ny, nz, ang, width=onx, thickness=onz, radial=w["radial"], log=True)
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        O.wbp_rows(p, proj, 0, nsl, nthreads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.wbp_rows(p, proj, 0, nsl, nthreads=cores)
+    dt = time.perf_counter() - t0
+    upd = float(onx) * onz * nsl * nz * args.steps
+    v = upd / dt
+    line = {"metric": METRIC, "value": v, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded counts)",
+            "impl": "reference",
+            "config": {"workload": "large plain WBP: 121 views 2048x2048 -> 2048x2048x800, RADIAL 0.35/0.035",
+                       "views": nz, "proj": [nx, ny], "volume": [onx, ny, onz], "parallelism": "host threads"},
+            "cpu_baseline": {"value": v, "unit": "updates/s", "cores": cores, "kind": "port",
+                             "sample": f"each step: slices 0..{nsl} (filter of their rows, stretch, WBP)"},
+            "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

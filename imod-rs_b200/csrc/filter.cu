@@ -1,0 +1,390 @@
+// filter.cu -- log transform, per-view means and the fused filter stage:
+// R-weighting (batched complex FFT of two packed real rows x radial weight x
+// inverse FFT), cosine stretch and packing into the staging format that the
+// back-projectors copy into shared memory.
+//
+// Reference semantics: apps/tilt/src/main.rs:333-381 (apply_rweighting),
+// 446-488 (apply_cosine_stretch, 411-441 cubic), 608-623 (log, means),
+// crates/imod-math/src/stats.rs:844-861 (min_max_mean).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "tg_internal.h"
+
+namespace tg {
+
+// ---------------------------------------------------------------------------
+// log10 (main.rs:608-613) fused with the per-view f64 sums (main.rs:616-623).
+// Grid (CH, nviews); every block owns a contiguous chunk of one view and
+// writes one f64 partial; a second kernel adds the CH partials in order, so
+// the result does not depend on scheduling.
+// ---------------------------------------------------------------------------
+constexpr int MEAN_CH = 32;
+
+__global__ void __launch_bounds__(256) log_sum_kernel(float *raw, long npix, int do_log,
+                                                      double *partials) {
+  const int v = blockIdx.y, c = blockIdx.x;
+  float *p = raw + (size_t)v * npix;
+  long c0 = npix * c / MEAN_CH, c1 = npix * (c + 1) / MEAN_CH;
+  double s = 0.0;
+  for (long i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+    float x = p[i];
+    if (do_log) {
+      // f32::max(0.001).log10(): computed in FP64 then rounded once
+      x = (float)log10((double)fmaxf(x, 0.001f));
+      p[i] = x;
+    }
+    s += (double)x;
+  }
+  __shared__ double red[8];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    partials[(size_t)v * MEAN_CH + c] = t;
+  }
+}
+
+__global__ void means_final_kernel(const double *partials, long npix, int nviews, float *means) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nviews) return;
+  double t = 0.0;
+  for (int c = 0; c < MEAN_CH; ++c) t += partials[(size_t)v * MEAN_CH + c];
+  means[v] = (float)(t / (double)npix);
+}
+
+void launch_log_means(float *raw, int npix, int nviews, int do_log, double *partials,
+                      float *means, cudaStream_t st) {
+  log_sum_kernel<<<dim3(MEAN_CH, nviews), 256, 0, st>>>(raw, npix, do_log, partials);
+  means_final_kernel<<<(nviews + 127) / 128, 128, 0, st>>>(partials, npix, nviews, means);
+}
+
+// ---------------------------------------------------------------------------
+// FFT plan: radices 4, 2, 3, 5, 7 (Stockham, auto-sorting).
+// ---------------------------------------------------------------------------
+bool fft_plan(int n, FftPlanDev *p) {
+  p->n = n;
+  p->nfac = 0;
+  int m = n;
+  while (m % 4 == 0) { p->fac[p->nfac++] = 4; m /= 4; }
+  while (m % 2 == 0) { p->fac[p->nfac++] = 2; m /= 2; }
+  for (int r : {3, 5, 7})
+    while (m % r == 0) { p->fac[p->nfac++] = r; m /= r; }
+  return m == 1 && p->nfac <= 24;
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV> __device__ __forceinline__ float2 rot(float2 a) {
+  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+template <int R, bool INV> __device__ __forceinline__ void bfly(float2 *v, const float2 *tw, int n) {
+  if constexpr (R == 2) {
+    float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (R == 4) {
+    float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    float2 b0 = cadd(v[1], v[3]), b1 = rot<INV>(csub(v[1], v[3]));
+    v[0] = cadd(a0, b0);
+    v[1] = cadd(a1, b1);
+    v[2] = csub(a0, b0);
+    v[3] = csub(a1, b1);
+  } else if constexpr (R == 3) {
+    const float s = 0.866025403784438646763723170752936183f;  // sin(2pi/3)
+    float2 t1 = cadd(v[1], v[2]);
+    float2 t2 = make_float2(v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y);
+    float2 d = csub(v[1], v[2]);
+    float2 t3 = rot<INV>(make_float2(s * d.x, s * d.y));
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(t2, t3);
+    v[2] = csub(t2, t3);
+  } else if constexpr (R == 5) {
+    const float c1 = 0.309016994374947424102293417182819059f;   // cos(2pi/5)
+    const float c2 = -0.809016994374947424102293417182819059f;  // cos(4pi/5)
+    const float s1 = 0.951056516295153572116439333379382143f;   // sin(2pi/5)
+    const float s2 = 0.587785252292473129168705954639072769f;   // sin(4pi/5)
+    float2 a1 = cadd(v[1], v[4]), a2 = cadd(v[2], v[3]);
+    float2 b1 = csub(v[1], v[4]), b2 = csub(v[2], v[3]);
+    float2 x0 = v[0];
+    float2 p1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+    float2 p2 = make_float2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+    float2 q1 = rot<INV>(make_float2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y));
+    float2 q2 = rot<INV>(make_float2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y));
+    v[0] = cadd(x0, cadd(a1, a2));
+    v[1] = cadd(p1, q1);
+    v[4] = csub(p1, q1);
+    v[2] = cadd(p2, q2);
+    v[3] = csub(p2, q2);
+  } else {  // generic (R = 7): direct DFT with table twiddles
+    float2 out[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      float2 acc = v[0];
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = __ldg(&tw[((r * j) % R) * (n / R)]);
+        if (INV) w.y = -w.y;
+        acc = cadd(acc, cmul(v[r], w));
+      }
+      out[j] = acc;
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j) v[j] = out[j];
+  }
+}
+
+// One Stockham pass of radix R: X -> Y, Ns = product of the radices done so far.
+template <int R, bool INV>
+__device__ __forceinline__ void stockham_pass(const float2 *X, float2 *Y, int n, int Ns,
+                                              const float2 *tw) {
+  const int nb = n / R;
+  const int tstride = n / (Ns * R);
+  for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+    int k = j % Ns;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = X[j + r * nb];
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = __ldg(&tw[r * k * tstride]);
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    bfly<R, INV>(v, tw, n);
+    int base = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) Y[base + r * Ns] = v[r];
+  }
+}
+
+// Full transform; returns the buffer holding the result.
+template <bool INV>
+__device__ float2 *stockham(float2 *A, float2 *B, const FftPlanDev &pl, const float2 *tw) {
+  int Ns = 1;
+  for (int i = 0; i < pl.nfac; ++i) {
+    int R = pl.fac[i];
+    switch (R) {
+      case 4: stockham_pass<4, INV>(A, B, pl.n, Ns, tw); break;
+      case 2: stockham_pass<2, INV>(A, B, pl.n, Ns, tw); break;
+      case 3: stockham_pass<3, INV>(A, B, pl.n, Ns, tw); break;
+      case 5: stockham_pass<5, INV>(A, B, pl.n, Ns, tw); break;
+      default: stockham_pass<7, INV>(A, B, pl.n, Ns, tw); break;
+    }
+    __syncthreads();
+    float2 *t = A; A = B; B = t;
+    Ns *= R;
+  }
+  return A;
+}
+
+// apps/tilt/src/main.rs:411-420 (Catmull-Rom), f32 operation order kept
+__device__ __forceinline__ float cubic1d(float p0, float p1, float p2, float p3, float t) {
+  float t2 = __fmul_rn(t, t);
+  float t3 = __fmul_rn(t2, t);
+  float a = __fadd_rn(__fsub_rn(__fadd_rn(__fmul_rn(-0.5f, p0), __fmul_rn(1.5f, p1)), __fmul_rn(1.5f, p2)), __fmul_rn(0.5f, p3));
+  float b = __fsub_rn(__fadd_rn(__fsub_rn(p0, __fmul_rn(2.5f, p1)), __fmul_rn(2.0f, p2)), __fmul_rn(0.5f, p3));
+  float c = __fadd_rn(__fmul_rn(-0.5f, p0), __fmul_rn(0.5f, p2));
+  return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(a, t3), __fmul_rn(b, t2)), __fmul_rn(c, t)), p1);
+}
+
+// Stretched sample at output column ox (main.rs:469-484, 425-441), zero outside.
+__device__ __forceinline__ float stretch_sample(const float *row, int nx, int ox, float stretch,
+                                                float center, int cubic) {
+  float dx = __fsub_rn((float)ox, center);
+  float src_x = __fadd_rn(__fmul_rn(dx, stretch), center);
+  float fl = floorf(src_x);
+  int sx0 = (int)fl;
+  if (fl < -1.0e9f) sx0 = -1000000000;  // far out of range: keep the int conversion safe
+  float frac = __fsub_rn(src_x, fl);
+  if (cubic && sx0 >= 1 && sx0 + 2 < nx) {
+    return cubic1d(row[sx0 - 1], row[sx0], row[sx0 + 1], row[sx0 + 2], frac);
+  }
+  if (sx0 >= 0 && sx0 + 1 < nx)
+    return __fadd_rn(__fmul_rn(row[sx0], __fsub_rn(1.0f, frac)), __fmul_rn(row[sx0 + 1], frac));
+  if (sx0 >= 0 && sx0 < nx) return row[sx0];
+  return 0.0f;
+}
+
+template <int STORE> struct Pack;
+template <> struct Pack<TG_STORE_FP16> {
+  static __device__ __forceinline__ uint32_t h2(float lo, float hi) {
+    __half2 h = __floats2half2_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&h);
+  }
+};
+template <> struct Pack<TG_STORE_BF16> {
+  static __device__ __forceinline__ uint32_t h2(float lo, float hi) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&h);
+  }
+};
+
+// Value pair (a, b) of element k of a final row, with the reference's fill
+// rule for samples whose left index is out of [0, nx-2] (main.rs:386-406).
+__device__ __forceinline__ void elem_ab(const float *row, int nx, int k, int fill_mode,
+                                        float fillv, float &a, float &b) {
+  if (k >= 0 && k + 1 < nx) {
+    a = row[k];
+    b = row[k + 1];
+  } else {
+    float f = fill_mode == TG_FILL_ZERO ? 0.0f
+              : fill_mode == TG_FILL_EDGE ? (k < 0 ? row[0] : row[nx - 1])
+                                          : fillv;
+    a = f;
+    b = f;
+  }
+}
+
+// One CTA per (row pair, view).  Rows 2j and 2j+1 are packed as the real and
+// imaginary part of one complex FFT: with a real, even weight the inverse
+// returns both filtered rows at once.
+template <int FMT, int STORE>
+__global__ void __launch_bounds__(256) filter_kernel(FilterArgs a) {
+  extern __shared__ __align__(16) unsigned char fsm[];
+  const int n = a.nx;
+  float2 *A = reinterpret_cast<float2 *>(fsm);
+  float2 *B = A + n;
+  const int jp = blockIdx.x, v = blockIdx.y;
+  const int r0 = 2 * jp, r1 = 2 * jp + 1;
+  const bool has1 = r1 < a.ny;
+  const float *in0 = a.in + ((size_t)v * a.ny + r0) * n;
+  const float *in1 = in0 + n;
+  const float *sb0 = a.sub ? a.sub + ((size_t)v * a.ny + r0) * n : nullptr;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    float x0 = in0[k], x1 = has1 ? in1[k] : 0.0f;
+    if (sb0) {  // SIRT residual: orig - reprojection (main.rs:933-935)
+      x0 = __fsub_rn(x0, sb0[k]);
+      if (has1) x1 = __fsub_rn(x1, sb0[n + k]);
+    }
+    A[k] = make_float2(x0, x1);
+  }
+  __syncthreads();
+  float2 *R = A;
+  if (a.weights) {
+    if (a.conv_h == nullptr) {
+      R = stockham<false>(A, B, a.plan, a.tw);
+      for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        float w = __ldg(&a.weights[k]);
+        float2 z = R[k];
+        R[k] = make_float2(__fmul_rn(z.x, w), __fmul_rn(z.y, w));
+      }
+      __syncthreads();
+      R = stockham<true>(R, R == A ? B : A, a.plan, a.tw);
+      for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        float2 z = R[k];
+        R[k] = make_float2(__fmul_rn(z.x, a.inv_n), __fmul_rn(z.y, a.inv_n));
+      }
+    } else {
+      // n without a radix-2/3/5/7 plan: circulant convolution with the
+      // inverse transform of the weights (h already includes 1/n).
+      for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        float s0 = 0.f, s1 = 0.f;
+        for (int m = 0; m < n; ++m) {
+          int d = k - m;
+          d += d < 0 ? n : 0;
+          float h = __ldg(&a.conv_h[d]);
+          float2 z = A[m];
+          s0 = fmaf(h, z.x, s0);
+          s1 = fmaf(h, z.y, s1);
+        }
+        B[k] = make_float2(s0, s1);
+      }
+      R = B;
+    }
+    __syncthreads();
+  }
+  // R holds the two filtered rows; un-interleave into float rows in the other buffer
+  float *row0 = reinterpret_cast<float *>(R == A ? B : A);
+  float *row1 = row0 + n;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    float2 z = R[k];
+    row0[k] = z.x;
+    row1[k] = z.y;
+  }
+  __syncthreads();
+  const float stretch = a.stretch ? a.stretch[v] : 0.0f;
+  if (stretch != 0.0f) {
+    float *s0 = reinterpret_cast<float *>(R);  // R is free now
+    float *s1 = s0 + n;
+    const float center = __fdiv_rn((float)n, 2.0f);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      s0[k] = stretch_sample(row0, n, k, stretch, center, a.cubic);
+      s1[k] = stretch_sample(row1, n, k, stretch, center, a.cubic);
+    }
+    __syncthreads();
+    row0 = s0;
+    row1 = s1;
+  }
+  const float fillv = a.fill ? a.fill[v] : 0.0f;
+  if (FMT == FMT_ROWPAIR) {
+    uint8_t *out = reinterpret_cast<uint8_t *>(a.out) +
+                   ((size_t)v * a.rows_alloc + jp) * (size_t)a.PW * (STORE == TG_STORE_FP32 ? 16 : 8);
+    for (int e = threadIdx.x; e < a.PW; e += blockDim.x) {
+      int k = e - a.padL;
+      float a0, b0, a1, b1;
+      elem_ab(row0, n, k, a.fill_mode, fillv, a0, b0);
+      if (has1) elem_ab(row1, n, k, a.fill_mode, fillv, a1, b1);
+      else a1 = b1 = 0.0f;
+      if (STORE == TG_STORE_FP32) {
+        reinterpret_cast<float4 *>(out)[e] = make_float4(a0, a1, b0, b1);
+      } else {
+        uint2 w;
+        w.x = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(a0, a1);
+        w.y = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(__fsub_rn(b0, a0), __fsub_rn(b1, a1));
+        reinterpret_cast<uint2 *>(out)[e] = w;
+      }
+    }
+  } else {
+    const int eb = STORE == TG_STORE_FP32 ? 8 : 4;
+    uint8_t *o0 = reinterpret_cast<uint8_t *>(a.out) + ((size_t)v * a.rows_alloc + r0) * (size_t)a.PW * eb;
+    uint8_t *o1 = o0 + (size_t)a.PW * eb;
+    for (int e = threadIdx.x; e < a.PW; e += blockDim.x) {
+      int k = e - a.padL;
+      float a0, b0;
+      elem_ab(row0, n, k, a.fill_mode, fillv, a0, b0);
+      float a1 = 0.f, b1 = 0.f;
+      if (has1) elem_ab(row1, n, k, a.fill_mode, fillv, a1, b1);
+      if (STORE == TG_STORE_FP32) {
+        reinterpret_cast<float2 *>(o0)[e] = make_float2(a0, b0);
+        if (has1) reinterpret_cast<float2 *>(o1)[e] = make_float2(a1, b1);
+      } else {
+        reinterpret_cast<uint32_t *>(o0)[e] =
+            Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(a0, __fsub_rn(b0, a0));
+        if (has1)
+          reinterpret_cast<uint32_t *>(o1)[e] =
+              Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(a1, __fsub_rn(b1, a1));
+      }
+    }
+  }
+}
+
+template <int FMT, int STORE> static void launch_f(const FilterArgs &a, cudaStream_t st) {
+  size_t smem = (size_t)a.nx * 16;  // two complex ping-pong buffers
+  auto k = filter_kernel<FMT, STORE>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k<<<dim3((a.ny + 1) / 2, a.nviews), 256, smem, st>>>(a);
+}
+
+void launch_filter(const FilterArgs &a, cudaStream_t st) {
+  if (a.fmt == FMT_ROWPAIR) {
+    if (a.store == TG_STORE_FP32) launch_f<FMT_ROWPAIR, TG_STORE_FP32>(a, st);
+    else if (a.store == TG_STORE_FP16) launch_f<FMT_ROWPAIR, TG_STORE_FP16>(a, st);
+    else launch_f<FMT_ROWPAIR, TG_STORE_BF16>(a, st);
+  } else {
+    if (a.store == TG_STORE_FP32) launch_f<FMT_SINGLE, TG_STORE_FP32>(a, st);
+    else if (a.store == TG_STORE_FP16) launch_f<FMT_SINGLE, TG_STORE_FP16>(a, st);
+    else launch_f<FMT_SINGLE, TG_STORE_BF16>(a, st);
+  }
+}
+
+}  // namespace tg

@@ -1,0 +1,131 @@
+// tg_internal.h -- shared declarations of libtiltgpu (kernels + host plumbing).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/tiltgpu.h"
+
+namespace tg {
+
+// Staged-projection formats written by the filter stage and read by the
+// back-projectors.  Element k of a row holds the samples needed to interpolate
+// anywhere in [k, k+1):
+//   FP32 : (row[k], row[k+1]); out-of-range k holds (fill, fill) and the
+//          kernel forces the fraction to 0 there, which reproduces the
+//          reference's `sample_row_with_fill` bit for bit.
+//   FP16/BF16 : (row[k], row[k+1]-row[k]); out-of-range k holds (fill, 0).
+// ROWPAIR interleaves rows 2j and 2j+1 of a view in one element
+// ([view][row-pair][PW]): FP32 float4 (a0, a1, b0, b1), FP16/BF16 uint2
+// (h2(a0,a1), h2(d0,d1)).  SINGLE keeps one row per element ([view][row][PW]):
+// FP32 float2 (a, b), FP16/BF16 uint32 h2(a, d).
+enum Fmt { FMT_ROWPAIR = 0, FMT_SINGLE = 1 };
+
+inline int elem_bytes(int fmt, int store) {
+  if (fmt == FMT_ROWPAIR) return store == TG_STORE_FP32 ? 16 : 8;
+  return store == TG_STORE_FP32 ? 8 : 4;
+}
+
+struct StatPartial {
+  float mn, mx;
+  double sum;
+};
+
+// ---- log transform + per-view means (main.rs:608-623) ----
+void launch_log_means(float *raw, int npix, int nviews, int do_log, double *partials,
+                      float *means, cudaStream_t st);
+
+// ---- filter stage: R-weighting (main.rs:333-381), cosine stretch
+// (main.rs:446-488) and staging-format packing ----
+struct FftPlanDev {
+  int n;
+  int nfac;
+  int fac[24];
+};
+bool fft_plan(int n, FftPlanDev *p);  // false if n has a prime factor > 7
+
+struct FilterArgs {
+  const float *in;          // [nviews_all][ny][nx]
+  const float *sub;         // optional: value = in - sub (SIRT residual)
+  void *out;                // staged format
+  const float *weights;     // n weights, nullptr = no R-weighting
+  const float2 *tw;         // n twiddles exp(-2 pi i k/n)
+  const float *conv_h;      // circulant kernel for n without a radix plan (else nullptr)
+  const float *stretch;     // per view 1/cos (f32) or 0: no stretch; nullptr = none
+  const float *fill;        // per view fill value for mean mode
+  int nx, ny, nviews;
+  int rows_alloc;           // rows (SINGLE) or row-pairs (ROWPAIR) per view in `out`
+  int PW, padL;
+  int fill_mode, cubic, fmt, store;
+  float inv_n;
+  FftPlanDev plan;
+};
+void launch_filter(const FilterArgs &a, cudaStream_t st);
+
+// ---- back-projection ----
+struct LocalDev {
+  // per view: offset into xs/ys (nxs, nys) and into grids; empty view: nxs=0
+  const int4 *vinfo;        // (x_off, nxs, y_off, nys)
+  const int *goff;          // grid offset per view
+  const float *xs, *ys, *gdx, *gdy;
+};
+struct BpArgs {
+  const void *pairs;
+  const float4 *vg;         // per view (cos_t, sin_t, zf, cos_xt)
+  const float4 *vg2;        // per view (sin_xt, 0, 0, 0)
+  float *vol;               // [ny][onz][onx]
+  StatPartial *partial;     // [ny][ntiles]
+  int *err;
+  int nx, ny, nviews, onx, onz;
+  int PW, padL, rows_alloc;
+  float cx, cz, ocx, inv_n, dw, os, oa, relax;
+  int mode;                 // 0: final (transform + stats), 1: store acc/N, 2: vol += relax*acc/N
+  int has_local;
+  LocalDev loc;
+};
+struct BpTile { int S, K, TX, NT, VPS, wmax; };
+// Fast kernel: no x-tilt, no local alignment, ROWPAIR format.
+int launch_bp_fast(const BpArgs &a, int store, bool zf, int variant, cudaStream_t st,
+                   int *ntiles_out);
+int bp_fast_variants();
+const char *bp_fast_variant_name(int v);
+// General kernel: x-tilt, z-factor, local alignment, SINGLE format.
+int launch_bp_general(const BpArgs &a, int store, cudaStream_t st, int *ntiles_out);
+int bp_fast_ntiles(const BpArgs &a, int variant);
+
+// ---- reprojection (main.rs:831-896) ----
+struct FpArgs {
+  const float *vol;         // [ny][onz][onx]
+  float *sino;              // [nviews_all][ny][nx] (views >= nviews are zeroed)
+  const float4 *vg, *vg2;
+  int nx, ny, nviews, nviews_all, onx, onz;
+  float cx, cz, ocx;
+  int has_local;
+  LocalDev loc;
+};
+void launch_reproject(const FpArgs &a, cudaStream_t st);
+
+// ---- volume operations ----
+void launch_lowpass(float *vol, float *tmp, int onx, int onz, int ny, cudaStream_t st);
+// in-place output transform + per-(slice, tile) partial stats
+void launch_transform_stats(float *vol, int onx, int onz, int ny, float dw, float os, float oa,
+                            StatPartial *partial, int *ntiles_out, cudaStream_t st);
+// per slice (min,max,mean) -> whole-volume stats in the reference's order
+void launch_stats_reduce(const StatPartial *partial, int ny, int ntiles, int slice_count,
+                         float *slice_stats, float *out3, cudaStream_t st);
+
+// ---- synthetic data ----
+int synth_projections(const tg_phantom_spec *spec, const float *angles, float *d_out,
+                      cudaStream_t st);
+
+// ---- errors ----
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+#define TG_CUDA(call)                                         \
+  do {                                                        \
+    cudaError_t _e = (call);                                  \
+    if (_e != cudaSuccess) return ::tg::cuda_fail(_e, #call); \
+  } while (0)
+
+}  // namespace tg

@@ -1,0 +1,368 @@
+// tilt_cli.cpp -- drop-in `tilt`: the reference's command line (clap Args of
+// apps/tilt/src/main.rs:18-120) plus IMOD PIP-style aliases, MRC in/out
+// byte-compatible with crates/imod-mrc, and the whole reconstruction on the
+// GPU through libtiltgpu's C ABI.
+//
+// Additions beyond the reference (documented in --help): the PIP aliases
+// -InputProjections -OutputFile -TILTFILE -THICKNESS -WIDTH -RADIAL
+// -SIRTIterations -LOG -SCALE -FakeSIRTiterations -XAXISTILT-file aliases are
+// mapped onto the same fields; --storage fp32|fp16|bf16 and --device N select
+// the staging precision and GPU.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cctype>
+#include <cerrno>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "mrc.h"
+#include "tiltgpu.h"
+
+namespace {
+
+struct Args {
+  std::string input, output, tilt_file;
+  int thickness = 0;
+  bool has_width = false;
+  int width = 0;
+  long threads = -1;
+  bool gpu = false;
+  std::string radial = "0.35,0.05";
+  bool no_weight = false;
+  long sirt = 0;
+  float sirt_relax = 1.0f;
+  bool no_cosine_stretch = false;
+  std::string local_file, xtilt_file, zfactor_file;
+  bool log = false;
+  float densweight = 1.0f, outscale = 1.0f, outadd = 0.0f;
+  long exact_filter_size = 0;
+  std::string fill_mode = "mean", cosine_interp = "linear";
+  float max_cosine_tilt = 80.0f;
+  bool hamming = false;
+  long fake_sirt = 0;
+  std::string storage = "fp32";
+  int device = 0;
+};
+
+void usage(FILE *f) {
+  fprintf(f,
+          "Weighted back-projection reconstruction (B200)\n\n"
+          "Usage: tilt [OPTIONS] --input <INPUT> --output <OUTPUT> --tilt-file <TILT_FILE>\n\n"
+          "Options:\n"
+          "  -i, --input <INPUT>              Input aligned tilt series (MRC)\n"
+          "  -o, --output <OUTPUT>            Output reconstruction (MRC)\n"
+          "  -t, --tilt-file <TILT_FILE>      Tilt angle file (.tlt)\n"
+          "  -z, --thickness <THICKNESS>      Thickness of output volume in Z (pixels) [default: 0]\n"
+          "  -w, --width <WIDTH>              Width of output (default: same as input)\n"
+          "  -j, --threads <THREADS>          Accepted for compatibility (all work is on the GPU)\n"
+          "      --gpu                        Semantics of the reference's wgpu back-projector\n"
+          "      --radial <RADIAL>            R-weighting cutoff,falloff [default: 0.35,0.05]\n"
+          "      --no-weight                  Disable R-weighting filter\n"
+          "      --sirt <SIRT>                Number of SIRT iterations (0 = plain WBP) [default: 0]\n"
+          "      --sirt-relax <SIRT_RELAX>    SIRT relaxation factor [default: 1]\n"
+          "      --no-cosine-stretch          Disable cosine stretching of projections\n"
+          "      --local-file <LOCAL_FILE>    Local alignment file (view x y dx dy per line)\n"
+          "      --xtilt-file <XTILT_FILE>    X-axis tilt file (one angle in degrees per view)\n"
+          "      --zfactor-file <ZFACTOR_FILE> Per-view Z scaling factor file\n"
+          "      --log                        Apply log10 to projection values first\n"
+          "      --densweight <DENSWEIGHT>    Density weight factor [default: 1]\n"
+          "      --outscale <OUTSCALE>        Output scale factor [default: 1]\n"
+          "      --outadd <OUTADD>            Output additive offset [default: 0]\n"
+          "      --exact-filter-size <N>      Radial filter table size\n"
+          "      --fill-mode <FILL_MODE>      mean, zero or edge [default: mean]\n"
+          "      --cosine-interp <MODE>       linear or cubic [default: linear]\n"
+          "      --max-cosine-tilt <DEG>      Max tilt for cosine stretching [default: 80]\n"
+          "      --hamming                    Hamming window instead of Gaussian rolloff\n"
+          "      --fake-sirt <N>              Low-pass smoothing passes [default: 0]\n"
+          "      --storage <fp32|fp16|bf16>   Staging precision of filtered projections (addition)\n"
+          "      --device <N>                 CUDA device ordinal (addition)\n"
+          "  -h, --help                       Print help\n\n"
+          "PIP-style aliases (additions): -InputProjections -OutputFile -TILTFILE -THICKNESS\n"
+          "  -WIDTH -RADIAL -SIRTIterations -LOG -SCALE <add,mult> -FakeSIRTiterations\n"
+          "  -XTILTFILE -ZFACTORFILE -LOCALFILE -HAMMING\n");
+}
+
+[[noreturn]] void clap_error(const std::string &msg) {
+  fprintf(stderr, "error: %s\n\nFor more information, try '--help'.\n", msg.c_str());
+  exit(2);
+}
+
+long parse_int(const std::string &v, const std::string &flag, bool allow_neg) {
+  char *end = nullptr;
+  errno = 0;
+  long x = strtol(v.c_str(), &end, 10);
+  if (v.empty() || end != v.c_str() + v.size() || errno || (!allow_neg && x < 0))
+    clap_error("invalid value '" + v + "' for '" + flag + "': invalid digit found in string");
+  return x;
+}
+float parse_float(const std::string &v, const std::string &flag) {
+  float x;
+  if (!mrc::parse_f32(v, x)) clap_error("invalid value '" + v + "' for '" + flag + "': invalid float literal");
+  return x;
+}
+
+std::string lower(std::string s) {
+  for (auto &c : s) c = (char)tolower((unsigned char)c);
+  return s;
+}
+
+Args parse(int argc, char **argv) {
+  Args a;
+  bool has_in = false, has_out = false, has_tlt = false;
+  // long flag -> canonical name; PIP aliases (case-insensitive) map here too
+  std::map<std::string, std::string> alias = {
+      {"-i", "input"}, {"--input", "input"}, {"-o", "output"}, {"--output", "output"},
+      {"-t", "tilt-file"}, {"--tilt-file", "tilt-file"}, {"-z", "thickness"}, {"--thickness", "thickness"},
+      {"-w", "width"}, {"--width", "width"}, {"-j", "threads"}, {"--threads", "threads"}};
+  std::map<std::string, std::string> pip = {
+      {"inputprojections", "input"}, {"inputfile", "input"}, {"outputfile", "output"},
+      {"tiltfile", "tilt-file"}, {"thickness", "thickness"}, {"width", "width"}, {"radial", "radial"},
+      {"sirtiterations", "sirt"}, {"log", "LOG"}, {"scale", "SCALE"}, {"fakesirtiterations", "fake-sirt"},
+      {"xtiltfile", "xtilt-file"}, {"zfactorfile", "zfactor-file"}, {"localfile", "local-file"},
+      {"hamming", "hamming"}, {"exactfiltersize", "exact-filter-size"}};
+  const std::vector<std::string> flags = {"gpu", "no-weight", "no-cosine-stretch", "log", "hamming"};
+  for (int i = 1; i < argc; ++i) {
+    std::string arg = argv[i], val;
+    bool has_eq = false;
+    if (arg == "-h" || arg == "--help") { usage(stdout); exit(0); }
+    std::string name;
+    if (arg.rfind("--", 0) == 0) {
+      size_t eq = arg.find('=');
+      if (eq != std::string::npos) { val = arg.substr(eq + 1); arg = arg.substr(0, eq); has_eq = true; }
+      auto it = alias.find(arg);
+      name = it != alias.end() ? it->second : arg.substr(2);
+    } else if (arg.size() == 2 && arg[0] == '-' && alias.count(arg)) {
+      name = alias[arg];
+    } else if (arg.size() > 2 && arg[0] == '-' && arg[1] != '-' && alias.count(arg.substr(0, 2)) &&
+               !pip.count(lower(arg.substr(1)))) {
+      name = alias[arg.substr(0, 2)];  // -z200 style
+      val = arg.substr(2);
+      has_eq = true;
+    } else if (arg.size() > 1 && arg[0] == '-' && pip.count(lower(arg.substr(1)))) {
+      name = pip[lower(arg.substr(1))];
+    } else {
+      clap_error("unexpected argument '" + arg + "' found");
+    }
+    bool is_flag = std::find(flags.begin(), flags.end(), name) != flags.end();
+    if (name == "LOG") {  // PIP LOG takes a value (an offset); any value turns the log on
+      if (i + 1 < argc && argv[i + 1][0] != '-') ++i;
+      a.log = true;
+      continue;
+    }
+    if (is_flag) {
+      if (has_eq) clap_error("unexpected value '" + val + "' for '--" + name + "' found; no more were expected");
+      if (name == "gpu") a.gpu = true;
+      else if (name == "no-weight") a.no_weight = true;
+      else if (name == "no-cosine-stretch") a.no_cosine_stretch = true;
+      else if (name == "log") a.log = true;
+      else if (name == "hamming") a.hamming = true;
+      continue;
+    }
+    if (!has_eq) {
+      if (i + 1 >= argc) clap_error("a value is required for '--" + name + "' but none was supplied");
+      val = argv[++i];
+    }
+    if (name == "input") { a.input = val; has_in = true; }
+    else if (name == "output") { a.output = val; has_out = true; }
+    else if (name == "tilt-file") { a.tilt_file = val; has_tlt = true; }
+    else if (name == "thickness") a.thickness = (int)parse_int(val, "--thickness", true);
+    else if (name == "width") { a.width = (int)parse_int(val, "--width", true); a.has_width = true; }
+    else if (name == "threads") a.threads = parse_int(val, "--threads", false);
+    else if (name == "radial") a.radial = val;
+    else if (name == "sirt") a.sirt = parse_int(val, "--sirt", false);
+    else if (name == "sirt-relax") a.sirt_relax = parse_float(val, "--sirt-relax");
+    else if (name == "local-file") a.local_file = val;
+    else if (name == "xtilt-file") a.xtilt_file = val;
+    else if (name == "zfactor-file") a.zfactor_file = val;
+    else if (name == "densweight") a.densweight = parse_float(val, "--densweight");
+    else if (name == "outscale") a.outscale = parse_float(val, "--outscale");
+    else if (name == "outadd") a.outadd = parse_float(val, "--outadd");
+    else if (name == "exact-filter-size") a.exact_filter_size = parse_int(val, "--exact-filter-size", false);
+    else if (name == "fill-mode") a.fill_mode = val;
+    else if (name == "cosine-interp") a.cosine_interp = val;
+    else if (name == "max-cosine-tilt") a.max_cosine_tilt = parse_float(val, "--max-cosine-tilt");
+    else if (name == "fake-sirt") a.fake_sirt = parse_int(val, "--fake-sirt", false);
+    else if (name == "storage") a.storage = lower(val);
+    else if (name == "device") a.device = (int)parse_int(val, "--device", false);
+    else if (name == "SCALE") {  // IMOD: (v + add) * mult == (v * mult) + add*mult
+      size_t c = val.find(',');
+      float add = parse_float(val.substr(0, c), "-SCALE");
+      float mult = c == std::string::npos ? 1.0f : parse_float(val.substr(c + 1), "-SCALE");
+      a.outscale = mult;
+      a.outadd = add * mult;
+    } else clap_error("unexpected argument '--" + name + "' found");
+  }
+  std::string missing;
+  if (!has_in) missing += "\n  --input <INPUT>";
+  if (!has_out) missing += "\n  --output <OUTPUT>";
+  if (!has_tlt) missing += "\n  --tilt-file <TILT_FILE>";
+  if (!missing.empty()) clap_error("the following required arguments were not provided:" + missing);
+  return a;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  Args args = parse(argc, argv);
+  std::string err;
+  std::vector<float> angles;
+  if (!mrc::read_tilt_file(args.tilt_file, angles, &err)) {  // main.rs:550-553
+    fprintf(stderr, "Error reading tilt file: %s\n", err.c_str());
+    return 1;
+  }
+  mrc::Reader reader;
+  if (!reader.open(args.input, &err)) {  // main.rs:555-558
+    fprintf(stderr, "Error: %s\n", err.c_str());
+    return 1;
+  }
+  const mrc::Header h = reader.header();
+  const int in_nx = h.nx, in_ny = h.ny, nz = h.nz;
+  const int out_nx = args.has_width ? args.width : h.nx;
+  const int out_ny = in_ny;
+  const int out_nz = args.thickness > 0 ? args.thickness : in_nx;
+  fprintf(stderr, "tilt: %d projections, %d x %d -> %d x %d x %d (B200)\n", nz, in_nx, in_ny, out_nx,
+          out_ny, out_nz);
+  // --radial: silently fall back to the defaults on parse failure (main.rs:580-585)
+  float cutoff = 0.35f, falloff = 0.05f;
+  {
+    std::vector<std::string> parts;
+    size_t s = 0;
+    while (true) {
+      size_t c = args.radial.find(',', s);
+      parts.push_back(args.radial.substr(s, c == std::string::npos ? std::string::npos : c - s));
+      if (c == std::string::npos) break;
+      s = c + 1;
+    }
+    auto tr = [](std::string x) {
+      size_t a = 0, b = x.size();
+      while (a < b && isspace((unsigned char)x[a])) ++a;
+      while (b > a && isspace((unsigned char)x[b - 1])) --b;
+      return x.substr(a, b - a);
+    };
+    float v;
+    if (parts.size() > 0 && mrc::parse_f32(tr(parts[0]), v)) cutoff = v;
+    if (parts.size() > 1 && mrc::parse_f32(tr(parts[1]), v)) falloff = v;
+  }
+  std::vector<float> proj((size_t)in_nx * in_ny * nz), sl;
+  for (int z = 0; z < nz; ++z) {
+    if (!reader.read_slice_f32(z, sl, &err) || sl.size() != (size_t)in_nx * in_ny) {
+      fprintf(stderr, "Error: %s\n", err.empty() ? "unsupported slice layout" : err.c_str());
+      return 1;
+    }
+    std::copy(sl.begin(), sl.end(), proj.begin() + (size_t)z * in_nx * in_ny);
+  }
+  std::vector<float> local_rows, xtilt, zfac;
+  if (!args.local_file.empty() && !mrc::load_local_rows(args.local_file, local_rows, &err)) {
+    fprintf(stderr, "Error reading local alignment file: %s\n", err.c_str());
+    return 1;
+  }
+  if (!args.xtilt_file.empty() && !mrc::load_per_view_file(args.xtilt_file, xtilt, &err)) {
+    fprintf(stderr, "Error reading xtilt file: %s\n", err.c_str());
+    return 1;
+  }
+  if (!args.zfactor_file.empty() && !mrc::load_per_view_file(args.zfactor_file, zfac, &err)) {
+    fprintf(stderr, "Error reading zfactor file: %s\n", err.c_str());
+    return 1;
+  }
+  tg_geometry g{};
+  g.nx = in_nx;
+  g.ny = in_ny;
+  g.nz = nz;
+  g.out_nx = out_nx;
+  g.out_nz = out_nz;
+  g.n_angles = (int)angles.size();
+  g.angles = angles.data();
+  if (!args.xtilt_file.empty()) { g.n_xtilt = (int)xtilt.size(); g.xtilt = xtilt.data(); }
+  if (!args.zfactor_file.empty()) { g.n_zfactor = (int)zfac.size(); g.zfactor = zfac.data(); }
+  if (!args.local_file.empty()) {
+    g.has_local = 1;
+    g.n_local = (int)(local_rows.size() / 5);
+    g.local = local_rows.data();
+  }
+  tg_options o;
+  tg_options_default(&o);
+  o.radial_cutoff = cutoff;
+  o.radial_falloff = falloff;
+  o.hamming = args.hamming;
+  o.exact_filter_size = (int)args.exact_filter_size;
+  o.no_weight = args.no_weight;
+  std::string fm = lower(args.fill_mode);
+  o.fill_mode = fm == "zero" ? TG_FILL_ZERO : fm == "edge" ? TG_FILL_EDGE : TG_FILL_MEAN;
+  o.no_cosine_stretch = args.no_cosine_stretch;
+  o.cosine_cubic = lower(args.cosine_interp) == "cubic";
+  o.max_cosine_tilt = args.max_cosine_tilt;
+  o.log_transform = args.log;
+  o.sirt_iters = (int)args.sirt;
+  o.sirt_relax = args.sirt_relax;
+  o.fake_sirt = (int)args.fake_sirt;
+  o.densweight = args.densweight;
+  o.outscale = args.outscale;
+  o.outadd = args.outadd;
+  o.gpu_compat = args.gpu;
+  o.storage = args.storage == "fp16" ? TG_STORE_FP16 : args.storage == "bf16" ? TG_STORE_BF16 : TG_STORE_FP32;
+  o.device = args.device;
+  tg_session *s = nullptr;
+  int rc = tg_session_create(&g, &o, &s);
+  if (rc == TG_ERR_PANIC) {  // the reference indexes tilt_angles out of bounds and panics
+    fprintf(stderr, "thread 'main' panicked: %s\n", tg_last_error());
+    return 101;
+  }
+  if (rc != TG_OK) {
+    fprintf(stderr, "Error: %s (%s)\n", tg_status_string(rc), tg_last_error());
+    return 1;
+  }
+  if ((rc = tg_upload_projections(s, proj.data(), proj.size())) != TG_OK || (rc = tg_reconstruct(s)) != TG_OK ||
+      (rc = tg_synchronize(s)) != TG_OK) {
+    fprintf(stderr, "Error: %s (%s)\n", tg_status_string(rc), tg_last_error());
+    tg_session_destroy(s);
+    return 1;
+  }
+  mrc::Header oh = mrc::Header::make(out_nx, out_nz, out_ny, mrc::FLOAT);  // main.rs:710-717
+  oh.xlen = h.xlen * (float)out_nx / (float)in_nx;
+  oh.ylen = h.xlen * (float)out_nz / (float)in_nx;
+  oh.zlen = h.ylen;
+  oh.mx = out_nx;
+  oh.my = out_nz;
+  oh.mz = out_ny;
+  oh.add_label("tilt: " + std::to_string(nz) + " projections, thickness " + std::to_string(out_nz));
+  mrc::Writer w;
+  if (!w.create(args.output, oh, &err)) {
+    fprintf(stderr, "Error: %s\n", err.c_str());
+    tg_session_destroy(s);
+    return 1;
+  }
+  const size_t slice = (size_t)out_nx * out_nz;
+  const int chunk = std::max(1, (int)std::min<size_t>(64, (256u << 20) / (slice * 4)));
+  std::vector<float> buf((size_t)chunk * slice);
+  tg_stats st{};
+  for (int y0 = 0; y0 < out_ny; y0 += chunk) {
+    int y1 = std::min(out_ny, y0 + chunk);
+    if ((rc = tg_download_slices(s, y0, y1, buf.data(), &st)) != TG_OK) {
+      fprintf(stderr, "Error: %s (%s)\n", tg_status_string(rc), tg_last_error());
+      tg_session_destroy(s);
+      return 1;
+    }
+    for (int y = y0; y < y1; ++y)
+      if (!w.write_slice_f32(buf.data() + (size_t)(y - y0) * slice, slice, &err)) {
+        fprintf(stderr, "Error: %s\n", err.c_str());
+        tg_session_destroy(s);
+        return 1;
+      }
+    fprintf(stderr, "  %d/%d rows\n", y1, out_ny);
+  }
+  tg_run_info info{};
+  tg_session_last_run(s, &info);
+  tg_session_destroy(s);
+  if (!w.finish(st.amin, st.amax, st.amean, &err)) {
+    fprintf(stderr, "Error: %s\n", err.c_str());
+    return 1;
+  }
+  fprintf(stderr, "tilt: reconstruction complete -> %s (%.3f ms on GPU, %.3g voxel-view updates/s)\n",
+          args.output.c_str(), info.ms_total, info.ms_total > 0 ? info.updates / (info.ms_total * 1e-3) : 0.0);
+  return 0;
+}

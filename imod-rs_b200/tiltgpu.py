@@ -1,0 +1,333 @@
+"""Python binding of libtiltgpu.so (the C ABI declared in include/tiltgpu.h).
+
+Mirrors the reference's `tilt` options (apps/tilt/src/main.rs:18-120) and its
+GPU seam (GpuSession::new / reconstruct_row, apps/tilt/src/gpu.rs:43-269).
+There is no CPU fallback: if the shared library is missing or no sm_100 GPU is
+present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libtiltgpu.so")
+CLI_PATH = os.path.join(_HERE, "bin", "tilt")
+
+TG_OK = 0
+STATUS = {0: "ok", -1: "invalid argument", -2: "out of device memory", -3: "CUDA error",
+          -4: "device wait timed out", -5: "over memory budget", -6: "unsupported",
+          -7: "no sm_100 CUDA device", -8: "input on which the reference panics",
+          -9: "not ready", -10: "not found"}
+FILL = {"mean": 0, "zero": 1, "edge": 2}
+STORAGE = {"fp32": 0, "fp16": 1, "bf16": 2}
+
+_f, _i32, _P = C.c_float, C.c_int32, C.c_void_p
+_fp = C.POINTER(C.c_float)
+
+
+class Geometry(C.Structure):
+    _fields_ = [("nx", _i32), ("ny", _i32), ("nz", _i32), ("out_nx", _i32), ("out_nz", _i32),
+                ("n_angles", _i32), ("angles", _fp), ("n_xtilt", _i32), ("xtilt", _fp),
+                ("n_zfactor", _i32), ("zfactor", _fp), ("n_local", _i32), ("local", _fp),
+                ("has_local", _i32)]
+
+
+class Options(C.Structure):
+    _fields_ = [("radial_cutoff", _f), ("radial_falloff", _f), ("hamming", _i32),
+                ("exact_filter_size", _i32), ("no_weight", _i32), ("fill_mode", _i32),
+                ("no_cosine_stretch", _i32), ("cosine_cubic", _i32), ("max_cosine_tilt", _f),
+                ("log_transform", _i32), ("sirt_iters", _i32), ("sirt_relax", _f),
+                ("fake_sirt", _i32), ("densweight", _f), ("outscale", _f), ("outadd", _f),
+                ("gpu_compat", _i32), ("storage", _i32), ("device", _i32), ("use_graphs", _i32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("amin", _f), ("amax", _f), ("amean", _f)]
+
+
+class RunInfo(C.Structure):
+    _fields_ = [("updates", C.c_double), ("ms_total", C.c_double), ("ms_filter", C.c_double),
+                ("ms_backproject", C.c_double), ("ms_reproject", C.c_double), ("passes", _i32),
+                ("kernel_launches", _i32)]
+
+
+class PhantomSpec(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("nx", _i32), ("ny", _i32), ("nz", _i32),
+                ("vol_nx", _i32), ("vol_nz", _i32), ("n_ell", _i32), ("rmin", _f), ("rmax", _f),
+                ("dmin", _f), ("dmax", _f), ("n_beads", _i32), ("bead_r", _f), ("bead_d", _f),
+                ("noise_kind", _i32), ("noise", _f), ("xtilt_deg", _f)]
+
+
+class TiltGpuError(RuntimeError):
+    def __init__(self, code, msg=""):
+        self.code = code
+        super().__init__(f"tiltgpu error {code} ({STATUS.get(code, '?')}): {msg}")
+
+
+EXPORTS = {
+    # name: (restype, argtypes)
+    "tg_abi_version": (C.c_int, []),
+    "tg_status_string": (C.c_char_p, [C.c_int]),
+    "tg_last_error": (C.c_char_p, []),
+    "tg_options_default": (None, [C.POINTER(Options)]),
+    "tg_session_create": (C.c_int, [C.POINTER(Geometry), C.POINTER(Options), C.POINTER(_P)]),
+    "tg_upload_projections": (C.c_int, [_P, _P, C.c_size_t]),
+    "tg_set_projections_device": (C.c_int, [_P, _P, C.c_size_t]),
+    "tg_reconstruct": (C.c_int, [_P]),
+    "tg_synchronize": (C.c_int, [_P]),
+    "tg_download_slices": (C.c_int, [_P, _i32, _i32, _P, C.POINTER(Stats)]),
+    "tg_get_stats": (C.c_int, [_P, C.POINTER(Stats)]),
+    "tg_volume_device": (_P, [_P]),
+    "tg_session_last_run": (C.c_int, [_P, C.POINTER(RunInfo)]),
+    "tg_session_dims": (C.c_int, [_P, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)]),
+    "tg_session_device_bytes": (C.c_size_t, [_P]),
+    "tg_session_destroy": (C.c_int, [_P]),
+    "tg_session_set_stream": (C.c_int, [_P, _P]),
+    "tg_gpu_session_new": (C.c_int, [_P, _P, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t,
+                                     C.c_size_t, _i32, C.POINTER(_P)]),
+    "tg_gpu_session_reconstruct_row": (C.c_int, [_P, C.c_size_t, _P]),
+    "tg_gpu_session_free": (None, [_P]),
+    "tg_apply_rweighting": (C.c_int, [_P, C.c_size_t, C.c_size_t, C.c_size_t, _f, _f, _i32,
+                                      _i32, _i32]),
+    "tg_synth_projections": (C.c_int, [C.POINTER(PhantomSpec), _P, _P, _i32, _i32]),
+}
+# library-internal helpers exported for tests and the benchmark (not in the header)
+EXTRA = {
+    "tg_session_kernel_info": (C.c_int, [_P, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32),
+                                         C.POINTER(_i32), C.POINTER(_i32)]),
+    "tg_session_set_variant": (C.c_int, [_P, _i32]),
+    "tg_variant_name": (C.c_char_p, [_i32]),
+}
+
+_lib = None
+
+
+def build(force=False):
+    """Compile libtiltgpu.so and bin/tilt with nvcc (cross-compiles without a GPU)."""
+    cmd = ["make", "-C", _HERE, "-j8"] + (["-B"] if force else [])
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is not built; run build() (make -C imod-rs_b200)")
+        _lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in {**EXPORTS, **EXTRA}.items():
+            fn = getattr(_lib, name)
+            fn.restype = res
+            fn.argtypes = args
+    return _lib
+
+
+def check(rc):
+    if rc != TG_OK:
+        raise TiltGpuError(rc, lib().tg_last_error().decode(errors="replace"))
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def _fptr(a):
+    return None if a is None else a.ctypes.data_as(_fp)
+
+
+def make_options(*, radial=(0.35, 0.05), hamming=False, exact_filter_size=None, no_weight=False,
+                 fill_mode="mean", no_cosine_stretch=False, cosine_interp="linear",
+                 max_cosine_tilt=80.0, log=False, sirt=0, sirt_relax=1.0, fake_sirt=0,
+                 densweight=1.0, outscale=1.0, outadd=0.0, gpu=False, storage="fp32", device=0,
+                 use_graphs=True) -> Options:
+    o = Options()
+    lib().tg_options_default(C.byref(o))
+    o.radial_cutoff, o.radial_falloff = float(radial[0]), float(radial[1])
+    o.hamming = int(bool(hamming))
+    o.exact_filter_size = int(exact_filter_size or 0)
+    o.no_weight = int(bool(no_weight))
+    o.fill_mode = FILL.get(str(fill_mode).lower(), 0)
+    o.no_cosine_stretch = int(bool(no_cosine_stretch))
+    o.cosine_cubic = int(str(cosine_interp).lower() == "cubic")
+    o.max_cosine_tilt = float(max_cosine_tilt)
+    o.log_transform = int(bool(log))
+    o.sirt_iters, o.sirt_relax, o.fake_sirt = int(sirt), float(sirt_relax), int(fake_sirt)
+    o.densweight, o.outscale, o.outadd = float(densweight), float(outscale), float(outadd)
+    o.gpu_compat = int(bool(gpu))
+    o.storage = STORAGE[storage] if isinstance(storage, str) else int(storage)
+    o.device, o.use_graphs = int(device), int(bool(use_graphs))
+    return o
+
+
+class Session:
+    """One tilt series resident on the device (tg_session_*)."""
+
+    def __init__(self, nx, ny, nz, angles, *, width=None, thickness=0, xtilt=None, zfactor=None,
+                 local=None, **opts):
+        self._keep = [_f32(angles), _f32(xtilt), _f32(zfactor),
+                      None if local is None else _f32(np.asarray(local).reshape(-1, 5))]
+        ang, xt, zf, loc = self._keep
+        g = Geometry()
+        g.nx, g.ny, g.nz = int(nx), int(ny), int(nz)
+        g.out_nx = int(width or 0)
+        g.out_nz = int(thickness or 0)
+        g.n_angles, g.angles = len(ang), _fptr(ang)
+        if xt is not None:
+            g.n_xtilt, g.xtilt = len(xt), _fptr(xt)
+        if zf is not None:
+            g.n_zfactor, g.zfactor = len(zf), _fptr(zf)
+        if loc is not None:
+            g.n_local, g.local, g.has_local = len(loc), _fptr(loc), 1
+        self.opts = make_options(**opts)
+        self.h = _P()
+        check(lib().tg_session_create(C.byref(g), C.byref(self.opts), C.byref(self.h)))
+        onx, onz, ony = _i32(), _i32(), _i32()
+        check(lib().tg_session_dims(self.h, C.byref(onx), C.byref(onz), C.byref(ony)))
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        self.out_shape = (ony.value, onz.value, onx.value)
+
+    def upload(self, proj):
+        p = _f32(proj)
+        check(lib().tg_upload_projections(self.h, _ptr(p), p.size))
+
+    def set_device(self, dev_ptr: int, n: int):
+        check(lib().tg_set_projections_device(self.h, _P(dev_ptr), n))
+
+    def reconstruct(self, sync=True):
+        check(lib().tg_reconstruct(self.h))
+        if sync:
+            check(lib().tg_synchronize(self.h))
+
+    def synchronize(self):
+        check(lib().tg_synchronize(self.h))
+
+    def download(self, y0=0, y1=None, out=None):
+        y1 = self.out_shape[0] if y1 is None else y1
+        shape = (y1 - y0,) + self.out_shape[1:]
+        if out is None:
+            out = np.empty(shape, np.float32)
+        st = Stats()
+        check(lib().tg_download_slices(self.h, y0, y1, _ptr(out), C.byref(st)))
+        return out, {"amin": st.amin, "amax": st.amax, "amean": st.amean}
+
+    def stats(self):
+        st = Stats()
+        check(lib().tg_get_stats(self.h, C.byref(st)))
+        return {"amin": st.amin, "amax": st.amax, "amean": st.amean}
+
+    def volume_ptr(self) -> int:
+        return lib().tg_volume_device(self.h)
+
+    def last_run(self):
+        ri = RunInfo()
+        check(lib().tg_session_last_run(self.h, C.byref(ri)))
+        return {k: getattr(ri, k) for k, _ in RunInfo._fields_}
+
+    def kernel_info(self):
+        vals = [_i32() for _ in range(5)]
+        check(lib().tg_session_kernel_info(self.h, *[C.byref(v) for v in vals]))
+        fast, variant, fmt, padl, pw = (v.value for v in vals)
+        return {"fast": bool(fast), "variant": variant,
+                "variant_name": lib().tg_variant_name(variant).decode() if fast else "general",
+                "fmt": fmt, "padL": padl, "PW": pw}
+
+    def set_variant(self, v: int):
+        check(lib().tg_session_set_variant(self.h, v))
+
+    def set_stream(self, stream_handle: int):
+        """Run on the caller's cudaStream_t (an integer handle; 0 = own stream)."""
+        check(lib().tg_session_set_stream(self.h, _P(stream_handle or None)))
+
+    def device_bytes(self):
+        return lib().tg_session_device_bytes(self.h)
+
+    def close(self):
+        if self.h:
+            lib().tg_session_destroy(self.h)
+            self.h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def reconstruct(proj, angles, **kw):
+    """One-shot: upload, reconstruct, download.  Returns (volume, stats)."""
+    nz, ny, nx = proj.shape
+    with Session(nx, ny, nz, angles, **kw) as s:
+        s.upload(proj)
+        s.reconstruct()
+        return s.download()
+
+
+class GpuSession:
+    """GpuSession::new / reconstruct_row of apps/tilt/src/gpu.rs, on the B200 kernels."""
+
+    def __init__(self, projections, tilt_cos_sin, in_nx, in_ny, n_projs, out_nx, out_nz, device=0):
+        self._p = _f32(projections)
+        self._cs = _f32(np.asarray(tilt_cos_sin).reshape(-1, 2))
+        self.out = (out_nz, out_nx)
+        self.h = _P()
+        check(lib().tg_gpu_session_new(_ptr(self._p), _ptr(self._cs), in_nx, in_ny, n_projs, out_nx,
+                                       out_nz, device, C.byref(self.h)))
+
+    def reconstruct_row(self, iy):
+        out = np.empty(self.out, np.float32)
+        check(lib().tg_gpu_session_reconstruct_row(self.h, iy, _ptr(out)))
+        return out
+
+    def close(self):
+        if self.h:
+            lib().tg_gpu_session_free(self.h)
+            self.h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def apply_rweighting(proj, cutoff=0.35, falloff=0.05, exact_filter_size=None, use_hamming=False,
+                     device=0):
+    """apply_rweighting (apps/tilt/src/main.rs:333) on the device; returns a new array."""
+    p = np.array(proj, dtype=np.float32, copy=True, order="C")
+    nz, ny, nx = p.shape
+    check(lib().tg_apply_rweighting(_ptr(p), nx, ny, nz, cutoff, falloff, int(exact_filter_size or 0),
+                                    int(use_hamming), device))
+    return p
+
+
+def synth_projections(angles, *, nx, ny, vol_nx=None, vol_nz, n_ell=300, rmin=3.0, rmax=40.0,
+                      dmin=0.2, dmax=1.0, n_beads=40, bead_r=5.0, bead_d=5.0, noise_kind=1,
+                      noise=0.5, xtilt_deg=0.0, seed=1, device=0, out_device_ptr=None):
+    """Seeded phantom projections [nz][ny][nx] (host array, or into a device pointer)."""
+    ang = _f32(angles)
+    sp = PhantomSpec()
+    sp.seed, sp.nx, sp.ny, sp.nz = int(seed), int(nx), int(ny), len(ang)
+    sp.vol_nx, sp.vol_nz = int(vol_nx or nx), int(vol_nz)
+    sp.n_ell, sp.rmin, sp.rmax, sp.dmin, sp.dmax = int(n_ell), rmin, rmax, dmin, dmax
+    sp.n_beads, sp.bead_r, sp.bead_d = int(n_beads), bead_r, bead_d
+    sp.noise_kind, sp.noise, sp.xtilt_deg = int(noise_kind), noise, xtilt_deg
+    if out_device_ptr is not None:
+        check(lib().tg_synth_projections(C.byref(sp), _ptr(ang), _P(out_device_ptr), 1, device))
+        return None
+    out = np.empty((len(ang), ny, nx), np.float32)
+    check(lib().tg_synth_projections(C.byref(sp), _ptr(ang), _ptr(out), 0, device))
+    return out

@@ -1,0 +1,221 @@
+/*
+ * tiltgpu.h -- C ABI of libtiltgpu.so, the B200 (sm_100a) implementation of the
+ * imod-rs `tilt` reconstruction path: R-weighted radial filtering of every
+ * projection row, cosine stretch, weighted back-projection with linear
+ * interpolation, and the SIRT reproject -> difference -> backproject loop, with
+ * projections and volume resident in device memory.
+ *
+ * Plain C types only (no CUDA or torch types cross this boundary).  Every
+ * function returns a tg_status (0 = TG_OK, negative = error); the library never
+ * falls back to a CPU implementation.  A session is single-thread-affine; the
+ * server object (tg_server_*) is thread-safe.
+ *
+ * Reference interfaces that each entry point replaces are cited as
+ * file:line inside the imod-rs project.
+ */
+#ifndef TILTGPU_H
+#define TILTGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TG_ABI_VERSION 1
+
+typedef enum {
+  TG_OK = 0,
+  TG_ERR_INVALID_ARG = -1,  /* bad sizes/pointers/options */
+  TG_ERR_OOM = -2,          /* device allocation failed */
+  TG_ERR_CUDA = -3,         /* a CUDA call failed (message via tg_last_error) */
+  TG_ERR_TIMEOUT = -4,      /* a bounded device wait gave up */
+  TG_ERR_BUDGET = -5,       /* job larger than the server's memory budget */
+  TG_ERR_UNSUPPORTED = -6,  /* option combination not implemented */
+  TG_ERR_NO_DEVICE = -7,    /* no CUDA device / not sm_100 */
+  TG_ERR_PANIC = -8,        /* input on which the reference panics (e.g. fewer
+                               tilt angles than views with cosine stretch on) */
+  TG_ERR_NOT_READY = -9,    /* tg_poll: job still running */
+  TG_ERR_NOT_FOUND = -10    /* unknown job id */
+} tg_status;
+
+/* Fill modes of apps/tilt/src/main.rs:122-128 */
+typedef enum { TG_FILL_MEAN = 0, TG_FILL_ZERO = 1, TG_FILL_EDGE = 2 } tg_fill_mode;
+
+/* Storage precision of the filtered projections staged for back-projection
+ * (accumulation is always FP32). */
+typedef enum { TG_STORE_FP32 = 0, TG_STORE_FP16 = 1, TG_STORE_BF16 = 2 } tg_storage;
+
+/* Geometry of one tilt series.  Replaces the dimension handling of
+ * apps/tilt/src/main.rs:560-571 and the per-view inputs of 550, 656-700. */
+typedef struct {
+  int32_t nx, ny, nz;        /* input stack: width, rows (tilt-axis direction), views */
+  int32_t out_nx;            /* output width  (--width);     <=0: nx  */
+  int32_t out_nz;            /* output thickness (-z);       <=0: nx  */
+  int32_t n_angles;          /* angles as read from the .tlt file (degrees, f32) */
+  const float *angles;
+  int32_t n_xtilt;           /* --xtilt-file values (degrees) or 0/NULL */
+  const float *xtilt;
+  int32_t n_zfactor;         /* --zfactor-file values or 0/NULL */
+  const float *zfactor;
+  int32_t n_local;           /* --local-file rows (view, x, y, dx, dy) or 0/NULL */
+  const float *local;
+  int32_t has_local;         /* --local-file given (even if it held no rows) */
+} tg_geometry;
+
+/* Options of apps/tilt/src/main.rs:18-120 (defaults via tg_options_default). */
+typedef struct {
+  float radial_cutoff;       /* --radial cutoff   (0.35) */
+  float radial_falloff;      /* --radial falloff  (0.05) */
+  int32_t hamming;           /* --hamming */
+  int32_t exact_filter_size; /* --exact-filter-size, <=0: none */
+  int32_t no_weight;         /* --no-weight */
+  int32_t fill_mode;         /* tg_fill_mode (--fill-mode) */
+  int32_t no_cosine_stretch; /* --no-cosine-stretch */
+  int32_t cosine_cubic;      /* --cosine-interp cubic */
+  float max_cosine_tilt;     /* --max-cosine-tilt (80) */
+  int32_t log_transform;     /* --log */
+  int32_t sirt_iters;        /* --sirt (0 = WBP) */
+  float sirt_relax;          /* --sirt-relax (1.0) */
+  int32_t fake_sirt;         /* --fake-sirt */
+  float densweight, outscale, outadd;  /* output transform (1, 1, 0) */
+  int32_t gpu_compat;        /* --gpu: semantics of apps/tilt/src/backproject.wgsl */
+  int32_t storage;           /* tg_storage of the staged filtered projections */
+  int32_t device;            /* CUDA device ordinal */
+  int32_t use_graphs;        /* capture each SIRT iteration in a CUDA graph (1) */
+} tg_options;
+
+/* Output header statistics (amin, amax, amean) of apps/tilt/src/main.rs:1077-1093 */
+typedef struct { float amin, amax, amean; } tg_stats;
+
+/* Per-call timing/accounting filled by tg_session_last_run. */
+typedef struct {
+  double updates;            /* voxel-view updates performed (onx*onz*ny*views per pass) */
+  double ms_total;           /* device time of the last tg_reconstruct (CUDA events) */
+  double ms_filter;          /* filter stage (R-weighting, stretch, staging format) */
+  double ms_backproject;     /* back-projection passes */
+  double ms_reproject;       /* SIRT reprojection passes */
+  int32_t passes;            /* back-projection passes (1 + sirt_iters) */
+  int32_t kernel_launches;   /* kernels launched by the last tg_reconstruct */
+} tg_run_info;
+
+typedef struct tg_session tg_session;
+
+void tg_options_default(tg_options *opt);
+const char *tg_status_string(int status);
+/* Message of the last error on this thread ("" if none). */
+const char *tg_last_error(void);
+int tg_abi_version(void);
+
+/* Replaces GpuSession::new (apps/tilt/src/gpu.rs:43-221) plus the CPU
+ * preprocessing of apps/tilt/src/main.rs:602-700: plans one tilt series and
+ * allocates its device buffers (projections, staged filtered rows, volume). */
+int tg_session_create(const tg_geometry *geom, const tg_options *opt, tg_session **out);
+/* Copies nx*ny*nz floats ([view][row][x], as read by MrcReader::read_slice_f32,
+ * crates/imod-mrc/src/read.rs:127-231) from host memory into the session. */
+int tg_upload_projections(tg_session *s, const float *host, size_t n);
+/* Same from device memory (cudaMemcpyDeviceToDevice on the session stream). */
+int tg_set_projections_device(tg_session *s, const float *dev, size_t n);
+/* Runs the whole path (log, means, R-weighting, stretch, WBP or SIRT, fake-SIRT,
+ * output transform, statistics) asynchronously on the session stream.
+ * Replaces the body of main() in apps/tilt/src/main.rs:607-1093. */
+int tg_reconstruct(tg_session *s);
+int tg_synchronize(tg_session *s);
+/* Copies output slices [y0, y1) ([y][out_nz][out_nx] f32) to host memory and
+ * returns the whole-volume header statistics. Synchronises the session. */
+int tg_download_slices(tg_session *s, int32_t y0, int32_t y1, float *host_out, tg_stats *stats);
+int tg_get_stats(tg_session *s, tg_stats *stats);
+/* Device pointer of the resident volume [ny][out_nz][out_nx]. */
+const float *tg_volume_device(tg_session *s);
+int tg_session_last_run(tg_session *s, tg_run_info *info);
+/* Resolved output dims (out_nx, out_nz, out_ny = ny). */
+int tg_session_dims(tg_session *s, int32_t *out_nx, int32_t *out_nz, int32_t *out_ny);
+/* Device bytes held by the session. */
+size_t tg_session_device_bytes(tg_session *s);
+/* Runs the session's work on the caller's CUDA stream (a cudaStream_t passed as
+ * void*; NULL restores the session's own stream).  No counterpart in the
+ * reference (its wgpu queue is private); lets a host runtime order the work
+ * with its own copies and timers. */
+int tg_session_set_stream(tg_session *s, void *cuda_stream);
+int tg_session_destroy(tg_session *s);
+
+/* ---- The reference's GPU seam, same arguments and meaning ----
+ * GpuSession::new(projections, tilt_cos_sin, in_nx, in_ny, n_projs, out_nx, out_nz)
+ * (apps/tilt/src/gpu.rs:43-51): projections are already filtered/stretched,
+ * tilt_cos_sin holds n_projs (cos, sin) pairs.  Returns TG_OK or an error
+ * where the reference returns None. */
+typedef struct tg_gpu_session tg_gpu_session;
+int tg_gpu_session_new(const float *projections, const float *tilt_cos_sin, size_t in_nx,
+                       size_t in_ny, size_t n_projs, size_t out_nx, size_t out_nz,
+                       int32_t device, tg_gpu_session **out);
+/* reconstruct_row(iy) (apps/tilt/src/gpu.rs:224-269): writes out_nx*out_nz floats. */
+int tg_gpu_session_reconstruct_row(tg_gpu_session *s, size_t iy, float *out);
+void tg_gpu_session_free(tg_gpu_session *s);
+
+/* ---- Stage function ----
+ * apply_rweighting(proj_data, in_nx, in_ny, nz, cutoff, falloff,
+ * exact_filter_size, use_hamming) (apps/tilt/src/main.rs:333): in place on a
+ * host array of in_nx*in_ny*nz floats, computed on the device. */
+int tg_apply_rweighting(float *proj_data, size_t in_nx, size_t in_ny, size_t nz, float cutoff,
+                        float falloff, int32_t exact_filter_size, int32_t use_hamming,
+                        int32_t device);
+
+/* ---- Synthetic seeded inputs (no counterpart in the reference; the
+ * workload generator for tests and benchmarks) ----
+ * Projects a seeded random ellipsoid phantom (n_ell ellipsoids with semi-axes
+ * in [rmin, rmax] px and densities U(dmin, dmax), plus n_beads spheres of
+ * radius bead_r and density bead_d) of size px_nx x ny x pz_nz along the given
+ * angles (degrees) with the reference geometry (x = dx*cos + dz*sin + nx/2,
+ * row = y), then adds noise:
+ *   noise_kind 0: none; 1: Gaussian with sigma = noise * std(signal);
+ *   2: counts = Poisson(noise * exp(-mu * line integral)) (noise = base
+ *      counts, mu = 1/pz_nz) written as counts, ready for --log.
+ * out: device or host pointer (is_device) of nz*ny*nx floats. */
+typedef struct {
+  uint64_t seed;
+  int32_t nx, ny, nz;         /* projection width, rows, views */
+  int32_t vol_nx, vol_nz;     /* phantom width and thickness (rows = ny) */
+  int32_t n_ell;
+  float rmin, rmax, dmin, dmax;
+  int32_t n_beads;
+  float bead_r, bead_d;
+  int32_t noise_kind;
+  float noise;
+  float xtilt_deg;            /* x-axis tilt of the projection geometry */
+} tg_phantom_spec;
+int tg_synth_projections(const tg_phantom_spec *spec, const float *angles, float *out,
+                         int32_t is_device, int32_t device);
+
+/* ---- MRC / tilt-file boundary (host only; usable without a GPU) ----
+ * Byte-compatible with crates/imod-mrc (header.rs:10-258, read.rs:28-231,
+ * write.rs:20-153) and crates/imod-transforms/src/tilt.rs:6-33. */
+typedef struct {
+  int32_t nx, ny, nz, mode, next;
+  int32_t swapped;           /* file was big-endian (MrcReader::is_swapped) */
+  float xlen, ylen, zlen;
+  float amin, amax, amean;
+  int32_t nlabl;
+  int32_t imod;              /* IMOD stamp present */
+  uint8_t header[1024];      /* the parsed header re-serialised little-endian */
+} tg_mrc_info;
+/* MrcHeader::new(nx, ny, nz, mode) serialised (header.rs:181-241), plus
+ * add_label(label) when label != NULL (header.rs:244-258). */
+int tg_mrc_header_new(int32_t nx, int32_t ny, int32_t nz, int32_t mode, const char *label,
+                      uint8_t out[1024]);
+/* MrcReader::open + read_slice_f32 for sections [z0, z1) (out may be NULL to
+ * read the header only).  out receives (z1-z0) * values-per-section floats. */
+int tg_mrc_read(const char *path, tg_mrc_info *info, int32_t z0, int32_t z1, float *out);
+/* MrcWriter::create(path, header) + write_slice_f32 for nsec sections +
+ * finish(amin, amax, amean).  header: 1024 little-endian bytes. */
+int tg_mrc_write_f32(const char *path, const uint8_t header[1024], const float *data,
+                     int32_t nsec, float amin, float amax, float amean);
+/* read_tilt_file: up to cap angles into out, count in *n. */
+int tg_read_tilt_file(const char *path, float *out, int32_t cap, int32_t *n);
+/* write_tilt_file ("{:10.2}" per line). */
+int tg_write_tilt_file(const char *path, const float *angles, int32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TILTGPU_H */
