@@ -12,6 +12,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <map>
 #include <mutex>
@@ -385,6 +386,21 @@ int tg_session_create(const tg_geometry *g, const tg_options *opt, tg_session **
   }
   if (g->n_angles < 1 || !g->angles) { set_error("no tilt angles"); return TG_ERR_INVALID_ARG; }
   if (opt->storage < 0 || opt->storage > 2) { set_error("bad storage"); return TG_ERR_INVALID_ARG; }
+  {
+    const int onx = g->out_nx > 0 ? g->out_nx : g->nx, onz = g->out_nz > 0 ? g->out_nz : g->nx;
+    if (onx > 65536 || onz > 65536) { set_error("output too large"); return TG_ERR_INVALID_ARG; }
+    // non-finite geometry would put sample positions outside every staged window
+    auto finite = [](const float *a, int n) {
+      for (int i = 0; a && i < n; ++i)
+        if (!std::isfinite(a[i])) return false;
+      return true;
+    };
+    if (!finite(g->angles, g->n_angles) || !finite(g->xtilt, g->n_xtilt) ||
+        !finite(g->zfactor, g->n_zfactor) || (g->local && !finite(g->local, 5 * g->n_local))) {
+      set_error("non-finite tilt, x-tilt, z-factor or local-alignment value");
+      return TG_ERR_INVALID_ARG;
+    }
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     set_error("no CUDA device");
