@@ -42,7 +42,20 @@ SMEM_BYTES_PER_CLK = 128  # per SM
 def c2_workload(jitter_seed=2):
     rng = np.random.default_rng(jitter_seed)
     ang = (np.arange(-60, 61, 1.0) + rng.normal(0.0, 0.1, 121)).astype(np.float32)
-    return dict(nx=2048, ny=2048, onx=2048, onz=800, angles=ang, radial=(0.35, 0.035))
+    return dict(name="large plain WBP: 121 views 2048x2048 -> 2048x2048x800, RADIAL 0.35/0.035",
+                nx=2048, ny=2048, onx=2048, onz=800, angles=ang, radial=(0.35, 0.035), n_ell=5000,
+                n_beads=200)
+
+
+def c1_workload():
+    """Config-1 shape, used for small profiling captures."""
+    ang = np.arange(-60, 61, 2.0).astype(np.float32)
+    return dict(name="plain WBP: 61 views 512x512 -> 512x512x200, RADIAL 0.35/0.035",
+                nx=512, ny=512, onx=512, onz=200, angles=ang, radial=(0.35, 0.035), n_ell=300,
+                n_beads=40)
+
+
+WORKLOADS = {"c2": c2_workload, "c1": c1_workload}
 
 
 class ClockSampler:
@@ -144,19 +157,22 @@ def run_ours(args):
 
     world, rank, local, dist = dist_setup(args)
     torch.cuda.set_device(local)
-    w = c2_workload()
+    w = WORKLOADS[args.workload]()
     nx, ny, onx, onz, ang = w["nx"], w["ny"], w["onx"], w["onz"], w["angles"]
     nz = len(ang)
     n_proj = nz * ny * nx
     # seeded phantom projections, generated on this rank's device (independent series per rank)
     proj_d = torch.empty(n_proj, dtype=torch.float32, device=f"cuda:{local}")
-    T.synth_projections(ang, nx=nx, ny=ny, vol_nx=onx, vol_nz=onz, n_ell=5000, rmin=3, rmax=40,
-                        dmin=0.2, dmax=1.0, n_beads=200, bead_r=5, bead_d=5.0, noise_kind=2,
+    T.synth_projections(ang, nx=nx, ny=ny, vol_nx=onx, vol_nz=onz, n_ell=w["n_ell"], rmin=3, rmax=40,
+                        dmin=0.2, dmax=1.0, n_beads=w["n_beads"], bead_r=5, bead_d=5.0, noise_kind=2,
                         noise=20000.0, seed=1000 + rank, device=local, out_device_ptr=proj_d.data_ptr())
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the session runs on it and the CUDA events below time it
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
     results = {}
     launches = 0
-    for form in ("fp32", "fp16"):
+    forms = [f for f in ("fp32", "fp16") if f in args.forms.split(",")]
+    for form in forms:
         s = T.Session(nx, ny, nz, ang, width=onx, thickness=onz, radial=w["radial"], log=True,
                       storage=form, device=local)
         s.set_stream(stream.cuda_stream)
@@ -199,6 +215,13 @@ def run_ours(args):
             sess16 = s
         else:
             s.close()
+    if args.profile:  # small-case profiling run: stage times only
+        if rank == 0:
+            print(json.dumps({f: {k: r[k] for k in ("ms", "bp_ms", "filter_ms")} | {"kernel": r["kernel"]}
+                              for f, r in results.items()}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     # ---- e2e through the public API with pinned host buffers
     s = sess16
     host_in = torch.empty(n_proj, dtype=torch.float32, pin_memory=True)
@@ -245,7 +268,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": r16["ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "storage": "fp16",
         "data": "synthetic (seeded ellipsoid+bead phantom, Poisson noise, --log)",
-        "config": {"workload": "large plain WBP: 121 views 2048x2048 -> 2048x2048x800, RADIAL 0.35/0.035",
+        "config": {"workload": w["name"],
                    "views": nz, "proj": [nx, ny], "volume": [onx, ny, onz],
                    "l2": "inputs larger than L2 (no flush needed)", "parallelism": f"replicas{world}",
                    "bp_kernel": r16["kernel"]["variant_name"]},
@@ -349,7 +372,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--forms", default="fp32,fp16", help="staging precisions to time")
+    ap.add_argument("--profile", action="store_true",
+                    help="time the requested forms only (no e2e, no CPU baseline); for ncu captures")
     args = ap.parse_args()
+    if not args.profile and set(args.forms.split(",")) != {"fp32", "fp16"}:
+        ap.error("--forms other than fp32,fp16 needs --profile")
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

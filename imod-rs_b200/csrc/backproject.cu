@@ -26,6 +26,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <type_traits>
+
 #include "tg_internal.h"
 #include "local_dev.cuh"
 
@@ -88,9 +90,52 @@ __device__ __forceinline__ float add_f32_bf16(float acc, uint16_t h) {
   return d;
 }
 
+// Packed FP32x2 arithmetic (PTX 8.6, sm_100+): two IEEE round-to-nearest f32
+// operations per instruction, each lane identical to the scalar operation.
+__device__ __forceinline__ uint64_t pk2(float lo, float hi) {
+  uint64_t d;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+  return d;
+}
+__device__ __forceinline__ float2 up2(uint64_t v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+// Shared loads at a 32-bit shared address plus a compile-time byte offset,
+// ordered after the mbarrier waits (all are volatile asm).
+template <int OFF> __device__ __forceinline__ float4 lds128i(uint32_t a) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4+%5];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"(a), "n"(OFF));
+  return v;
+}
+template <int OFF> __device__ __forceinline__ uint2 lds64i(uint32_t a) {
+  uint2 v;
+  asm volatile("ld.shared.v2.u32 {%0,%1}, [%2+%3];" : "=r"(v.x), "=r"(v.y) : "r"(a), "n"(OFF));
+  return v;
+}
+template <int I, int N, class F> __device__ __forceinline__ void static_for(F &&f) {
+  if constexpr (I < N) {
+    f(std::integral_constant<int, I>{});
+    static_for<I + 1, N>(f);
+  }
+}
+
 constexpr float MAGIC = 12582912.0f;      // 1.5 * 2^23
 constexpr uint32_t MAGIC_BITS = 0x4B400000u;
-constexpr long WAIT_LIMIT = 1L << 26;     // bounded spin on an mbarrier phase
 
 // exact reference position for (dx, dz): ((dx*c)*cxt + (dz*s)*zf) + cx
 template <bool ZF>
@@ -100,21 +145,62 @@ __device__ __forceinline__ float ref_x(float t1, float dz, float s, float zf, fl
   return __fadd_rn(__fadd_rn(t1, t2), cx);
 }
 
-template <int STORE, int S, int K, int TX, int NT, int VPS, bool ZF>
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
 struct FastCfg {
-  static constexpr int SP = S / 2;
-  static constexpr int OZG = NT / TX;
-  static constexpr int TZ = OZG * K;
+  static constexpr int SP = S / 2;           // row pairs per tile
+  static constexpr int OZG = NT / TX;        // depth groups of consumer threads
+  static constexpr int TZ = OZG * K;         // tile depth
+  static constexpr int NTHR = NT + 32;       // consumers + one producer warp
   static constexpr int EB = STORE == TG_STORE_FP32 ? 16 : 8;
-  static constexpr int WMAX = ((TX + TZ * (ZF ? 2 : 1) + 8) + 1) & ~1;  // elements, even
+  static constexpr int WMAX = ((TX + TZ * (ZF ? 2 : 1) + 8) + 1) & ~1;  // window elements, even
   static constexpr int SLOT = SP * WMAX * EB;                             // bytes per view
-  static constexpr int BUF = 2 * VPS * SLOT;
-  static size_t smem(int nviews) { return BUF + 8 * (size_t)nviews + 16 + 16 * (NT / 32) * S + 64; }
+  static constexpr int BUF = NSTAGE * VPS * SLOT;
+  static_assert(VPS * SP <= 32, "one copy per producer lane");
+  static size_t smem(int nviews) { return BUF + 8 * (size_t)nviews + 16 * NSTAGE + 16 + 64; }
 };
 
-template <int STORE, int S, int K, int TX, int NT, int VPS, bool ZF>
-__global__ void __launch_bounds__(NT) bp_fast_kernel(BpArgs a) {
-  using C = FastCfg<STORE, S, K, TX, NT, VPS, ZF>;
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void consumer_sync(int nthreads) {
+  asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+// try_wait that lets the hardware suspend the thread (up to hint_ns) until the
+// phase completes, instead of returning at once
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s: a stage never legitimately takes this long
+// Bounded wait on an mbarrier phase: sleeps in try_wait, gives up after
+// WAIT_LIMIT_NS of wall time or when another warp of the CTA has given up.
+__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t parity, volatile int *abort) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (;;) {
+    if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
+    if (*abort || globaltimer_ns() - t0 > WAIT_LIMIT_NS) return false;
+  }
+}
+
+// Warp-specialised pipeline: warp NT/32 (the producer) copies each stage's
+// per-view row windows with cp.async.bulk, one copy per lane, completing on
+// full[b]; consumer warps wait on full[b], accumulate, and release the buffer
+// on empty[b].  NSTAGE buffers of VPS views form a ring.
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
+__global__ void __launch_bounds__(NT + 32) bp_fast_kernel(BpArgs a) {
+  using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   constexpr int SP = C::SP, OZG = C::OZG, TZ = C::TZ, EB = C::EB, WMAX = C::WMAX, SLOT = C::SLOT;
   extern __shared__ __align__(128) unsigned char sm[];
   unsigned char *bufs = sm;
@@ -122,17 +208,16 @@ __global__ void __launch_bounds__(NT) bp_fast_kernel(BpArgs a) {
   int *win_n = win_k0 + a.nviews;
   uint64_t *bars = reinterpret_cast<uint64_t *>(
       (reinterpret_cast<uintptr_t>(win_n + a.nviews) + 15) & ~(uintptr_t)15);
-  __shared__ int s_abort;
+  uint64_t *full = bars, *empty = bars + NSTAGE;
+  __shared__ volatile int s_abort;
 
   const int tid = threadIdx.x;
-  const int tx = tid % TX, tzg = tid / TX;
   const int ox0 = blockIdx.x * TX, oz0 = blockIdx.y * TZ, iy0 = blockIdx.z * S;
-  const int ox = min(ox0 + tx, a.onx - 1);
   const int oxlo = ox0, oxhi = min(ox0 + TX, a.onx) - 1;
   const int ozlo = oz0, ozhi = min(oz0 + TZ, a.onz) - 1;
 
-  // ---- per-view windows of this tile (corners bound x: it is monotone in dx and dz)
-  for (int v = tid; v < a.nviews; v += NT) {
+  // ---- per-view windows of this tile (x is monotone in dx and dz: corners bound it)
+  for (int v = tid; v < a.nviews; v += C::NTHR) {
     float4 g = __ldg(&a.vg[v]);
     float t1l = __fmul_rn(__fsub_rn((float)oxlo, a.ocx), g.x);
     float t1h = __fmul_rn(__fsub_rn((float)oxhi, a.ocx), g.x);
@@ -156,67 +241,94 @@ __global__ void __launch_bounds__(NT) bp_fast_kernel(BpArgs a) {
     win_n[v] = cnt;
   }
   if (tid == 0) {
-    mbar_init(smem_u32(&bars[0]), 1);
-    mbar_init(smem_u32(&bars[1]), 1);
+    for (int b = 0; b < NSTAGE; ++b) {
+      mbar_init(smem_u32(&full[b]), 1);
+      mbar_init(smem_u32(&empty[b]), NT / 32);
+    }
     fence_mbar_init();
     s_abort = 0;
   }
   __syncthreads();
 
   const int nst = (a.nviews + VPS - 1) / VPS;
-  const uint8_t *pairs = reinterpret_cast<const uint8_t *>(a.pairs);
-  const int jp0 = iy0 / 2;
-  auto issue = [&](int st) {
-    const int v0 = st * VPS, nv = min(VPS, a.nviews - v0);
-    const uint32_t bar = smem_u32(&bars[st & 1]);
-    uint32_t bytes = 0;
-    for (int vi = 0; vi < nv; ++vi) bytes += (uint32_t)(SP * win_n[v0 + vi] * EB);
-    fence_proxy_async();
-    mbar_expect_tx(bar, bytes);
-    for (int vi = 0; vi < nv; ++vi) {
-      const int v = v0 + vi, k0 = win_k0[v], n = win_n[v];
-      const uint32_t dst = smem_u32(bufs) + ((st & 1) * VPS + vi) * SLOT;
-      for (int sp = 0; sp < SP; ++sp) {
-        const uint8_t *src =
-            pairs + (((size_t)v * a.rows_alloc + jp0 + sp) * a.PW + (size_t)(k0 + a.padL)) * EB;
-        bulk_g2s(dst + sp * WMAX * EB, src, (uint32_t)(n * EB), bar);
+  if (tid >= NT) {
+    // ---------------- producer warp ----------------
+    const int lane = tid - NT;
+    const uint8_t *pairs = reinterpret_cast<const uint8_t *>(a.pairs);
+    const int jp0 = iy0 / 2;
+    int issued = 0;
+    for (int st = 0; st < nst; ++st) {
+      const int b = st % NSTAGE;
+      if (st >= NSTAGE && !wait_phase(smem_u32(&empty[b]), ((st / NSTAGE) - 1) & 1, &s_abort)) {
+        s_abort = 1;
+        break;
       }
+      if (s_abort) break;
+      const int v0 = st * VPS, nv = min(VPS, a.nviews - v0);
+      const bool mine = lane < nv * SP;
+      const int vi = lane / SP, sp = lane % SP, v = v0 + vi;
+      const uint32_t bytes = mine ? (uint32_t)(win_n[v] * EB) : 0u;
+      const uint32_t total = __reduce_add_sync(0xffffffffu, bytes);
+      if (lane == 0) {
+        fence_proxy_async();  // order the consumers' reads of buffer b before the refill
+        mbar_expect_tx(smem_u32(&full[b]), total);
+      }
+      __syncwarp();
+      if (mine) {
+        const uint8_t *src =
+            pairs + (((size_t)v * a.rows_alloc + jp0 + sp) * a.PW + (size_t)(win_k0[v] + a.padL)) * EB;
+        const uint32_t dst = smem_u32(bufs) + (b * VPS + vi) * SLOT + sp * WMAX * EB;
+        bulk_g2s(dst, src, bytes, smem_u32(&full[b]));
+      }
+      ++issued;
     }
-  };
+    // no copy may still be landing when the CTA exits: bounded wait on the last stages
+    if (lane == 0)
+      for (int st = max(0, issued - NSTAGE); st < issued; ++st)
+        wait_phase(smem_u32(&full[st % NSTAGE]), (st / NSTAGE) & 1, &s_abort);
+    return;
+  }
 
-  float acc[S][K];
+  // ---------------- consumer warps ----------------
+  const int tx = tid % TX, tzg = tid / TX;
+  const int ox = min(ox0 + tx, a.onx - 1);
+  // FP32: accumulators of slices (2sp, 2sp+1) packed for the f32x2 pipe;
+  // FP16/BF16: one f32 accumulator per slice
+  constexpr int NACC = STORE == TG_STORE_FP32 ? 1 : S;
+  constexpr int NACC2 = STORE == TG_STORE_FP32 ? SP : 1;
+  float acc[NACC][K];
+  uint64_t acc2[NACC2][K];
 #pragma unroll
-  for (int s = 0; s < S; ++s)
+  for (int j = 0; j < K; ++j) {
 #pragma unroll
-    for (int j = 0; j < K; ++j) acc[s][j] = 0.0f;
+    for (int s = 0; s < NACC; ++s) acc[s][j] = 0.0f;
+#pragma unroll
+    for (int s = 0; s < NACC2; ++s) acc2[s][j] = 0ull;
+  }
   const float dx = __fsub_rn((float)ox, a.ocx);
   float dz[K];
 #pragma unroll
   for (int j = 0; j < K; ++j) dz[j] = __fsub_rn((float)min(oz0 + tzg + j * OZG, a.onz - 1), a.cz);
 
-  if (tid == 0 && nst > 0) issue(0);
-  for (int st = 0; st < nst; ++st) {
-    if (tid == 0 && st + 1 < nst) issue(st + 1);
-    {
-      const uint32_t bar = smem_u32(&bars[st & 1]);
-      const uint32_t par = (st >> 1) & 1;
-      long spins = 0;
-      while (!mbar_try_wait(bar, par)) {
-        if (++spins > WAIT_LIMIT) {
-          s_abort = 1;
-          break;
-        }
-      }
+  bool ok = true;
+  for (int st = 0; st < nst && ok; ++st) {
+    const int b = st % NSTAGE;
+    if (!wait_phase(smem_u32(&full[b]), (st / NSTAGE) & 1, &s_abort)) {
+      s_abort = 1;
+      ok = false;
+      break;
     }
-    if (!s_abort) {
-      const int v0 = st * VPS, nv = min(VPS, a.nviews - v0);
-      for (int vi = 0; vi < nv; ++vi) {
+    const int v0 = st * VPS, nv = min(VPS, a.nviews - v0);
+#pragma unroll
+    for (int vi = 0; vi < VPS; ++vi) {
+      if (vi < nv) {
         const int v = v0 + vi;
         const float4 g = __ldg(&a.vg[v]);
         const float t1 = __fmul_rn(dx, g.x);  // (dx*cos_t)*cos_xt, cos_xt == 1 exactly here
         const int k0 = win_k0[v];
-        const uint32_t slot = smem_u32(bufs) + ((st & 1) * VPS + vi) * SLOT;
-        const uint32_t adj = slot - (MAGIC_BITS + (uint32_t)k0) * (uint32_t)EB;
+        // shared address of element k of this view's slot: bits(tt)*EB + adj
+        const uint32_t adj = smem_u32(bufs) + (uint32_t)((b * VPS + vi) * SLOT) -
+                             (MAGIC_BITS + (uint32_t)k0) * (uint32_t)EB;
 #pragma unroll
         for (int j = 0; j < K; ++j) {
           const float x = ref_x<ZF>(t1, dz[j], g.y, g.z, a.cx);
@@ -228,53 +340,49 @@ __global__ void __launch_bounds__(NT) bp_fast_kernel(BpArgs a) {
             const bool in = (bits - MAGIC_BITS) <= (uint32_t)(a.nx - 2);
             const float f = in ? f0 : 0.0f;
             const float omf = __fsub_rn(1.0f, f);
-#pragma unroll
-            for (int sp = 0; sp < SP; ++sp) {
-              const float4 e = lds128(addr + sp * WMAX * 16);
-              acc[2 * sp][j] = __fadd_rn(acc[2 * sp][j], __fadd_rn(__fmul_rn(e.x, omf), __fmul_rn(e.z, f)));
-              acc[2 * sp + 1][j] =
-                  __fadd_rn(acc[2 * sp + 1][j], __fadd_rn(__fmul_rn(e.y, omf), __fmul_rn(e.w, f)));
-            }
+            const uint64_t omf2 = pk2(omf, omf), ff2 = pk2(f, f);
+            static_for<0, SP>([&](auto spc) {
+              constexpr int sp = decltype(spc)::value;
+              // (a0, a1, b0, b1): RN(RN(a*(1-f)) + RN(b*f)) for both slices.  The
+              // products use the f32x2 pipe; the sums stay scalar so that no
+              // multiply is contracted into them.
+              const float4 e = lds128i<sp * WMAX * 16>(addr);
+              const float2 p = up2(mul2(pk2(e.x, e.y), omf2));
+              const float2 q = up2(mul2(pk2(e.z, e.w), ff2));
+              acc2[sp][j] = add2(acc2[sp][j], pk2(__fadd_rn(p.x, q.x), __fadd_rn(p.y, q.y)));
+            });
           } else if constexpr (STORE == TG_STORE_FP16) {
             const __half2 f2 = __float2half2_rn(f0);
-#pragma unroll
-            for (int sp = 0; sp < SP; ++sp) {
-              const uint2 e = lds64(addr + sp * WMAX * 8);
+            static_for<0, SP>([&](auto spc) {
+              constexpr int sp = decltype(spc)::value;
+              const uint2 e = lds64i<sp * WMAX * 8>(addr);
               const __half2 r = __hfma2(f2, *reinterpret_cast<const __half2 *>(&e.y),
                                         *reinterpret_cast<const __half2 *>(&e.x));
               const uint32_t rb = *reinterpret_cast<const uint32_t *>(&r);
               acc[2 * sp][j] = add_f32_f16(acc[2 * sp][j], (uint16_t)(rb & 0xffffu));
               acc[2 * sp + 1][j] = add_f32_f16(acc[2 * sp + 1][j], (uint16_t)(rb >> 16));
-            }
+            });
           } else {
             const __nv_bfloat162 f2 = __float2bfloat162_rn(f0);
-#pragma unroll
-            for (int sp = 0; sp < SP; ++sp) {
-              const uint2 e = lds64(addr + sp * WMAX * 8);
+            static_for<0, SP>([&](auto spc) {
+              constexpr int sp = decltype(spc)::value;
+              const uint2 e = lds64i<sp * WMAX * 8>(addr);
               const __nv_bfloat162 r = __hfma2(f2, *reinterpret_cast<const __nv_bfloat162 *>(&e.y),
                                                *reinterpret_cast<const __nv_bfloat162 *>(&e.x));
               const uint32_t rb = *reinterpret_cast<const uint32_t *>(&r);
               acc[2 * sp][j] = add_f32_bf16(acc[2 * sp][j], (uint16_t)(rb & 0xffffu));
               acc[2 * sp + 1][j] = add_f32_bf16(acc[2 * sp + 1][j], (uint16_t)(rb >> 16));
-            }
+            });
           }
         }
       }
     }
-    __syncthreads();
-    if (s_abort) break;
+    __syncwarp();
+    if ((tid & 31) == 0) mbar_arrive(smem_u32(&empty[b]));  // this warp is done with buffer b
   }
+  consumer_sync(NT);  // all consumers past the loop (buffers free, abort flag settled)
   if (s_abort) {
-    if (tid == 0) {
-      atomicOr(a.err, 1);
-      // bounded drain of copies still in flight on either barrier before the CTA exits
-      for (int b = 0; b < 2; ++b) {
-        long spins = 0;
-        while (!mbar_try_wait(smem_u32(&bars[b]), 0) && !mbar_try_wait(smem_u32(&bars[b]), 1) &&
-               ++spins < WAIT_LIMIT) {
-        }
-      }
-    }
+    if (tid == 0) atomicOr(a.err, 1);
     return;
   }
 
@@ -293,7 +401,14 @@ __global__ void __launch_bounds__(NT) bp_fast_kernel(BpArgs a) {
       const int oz = oz0 + tzg + j * OZG;
       if (xok && oz < a.onz && iy < a.ny) {
         const size_t idx = ((size_t)iy * a.onz + oz) * a.onx + oxr;
-        const float v = __fmul_rn(acc[s][j], a.inv_n);
+        float accv;
+        if constexpr (STORE == TG_STORE_FP32) {
+          const float2 p = up2(acc2[s / 2][j]);
+          accv = (s & 1) ? p.y : p.x;
+        } else {
+          accv = acc[s < NACC ? s : 0][j];
+        }
+        const float v = __fmul_rn(accv, a.inv_n);
         if (a.mode == 0) {
           const float y = __fadd_rn(__fmul_rn(__fmul_rn(v, a.dw), a.os), a.oa);
           a.vol[idx] = y;
@@ -322,7 +437,7 @@ __global__ void __launch_bounds__(NT) bp_fast_kernel(BpArgs a) {
     }
   }
   if (a.mode == 0) {
-    __syncthreads();
+    consumer_sync(NT);
     if (tid < S && iy0 + tid < a.ny) {
       float mn = 3.40282347e+38f, mx = -3.40282347e+38f;
       double sum = 0.0;
@@ -342,39 +457,45 @@ __global__ void __launch_bounds__(NT) bp_fast_kernel(BpArgs a) {
 }
 
 // ---- variant table (tile shapes the autotuner chooses from) ----
-struct FastVariant { int S, K, TX, NT, VPS; const char *name; };
+struct FastVariant { int S, K, TX, NT, VPS, NSTAGE; const char *name; };
 static const FastVariant kFast[] = {
-    {8, 4, 64, 256, 4, "S8K4TX64NT256"},
-    {8, 8, 64, 256, 2, "S8K8TX64NT256"},
-    {8, 4, 32, 128, 4, "S8K4TX32NT128"},
-    {4, 8, 64, 256, 4, "S4K8TX64NT256"},
-    {8, 2, 128, 256, 4, "S8K2TX128NT256"},
+    {8, 4, 32, 128, 2, 4, "S8K4TX32NT128V2N4"},
+    {8, 4, 32, 128, 4, 3, "S8K4TX32NT128V4N3"},
+    {8, 4, 32, 256, 2, 4, "S8K4TX32NT256V2N4"},
+    {8, 4, 64, 256, 2, 4, "S8K4TX64NT256V2N4"},
+    {16, 2, 32, 128, 2, 4, "S16K2TX32NT128V2N4"},
+    {16, 2, 32, 256, 2, 4, "S16K2TX32NT256V2N4"},
+    {8, 8, 32, 128, 2, 4, "S8K8TX32NT128V2N4"},
 };
+constexpr int MAX_S = 16;  // rows per tile of the widest variant (sizes the staging buffer)
 int bp_fast_variants() { return (int)(sizeof(kFast) / sizeof(kFast[0])); }
 const char *bp_fast_variant_name(int v) { return kFast[v].name; }
+int bp_fast_row_align() { return MAX_S; }
 
-template <int STORE, int S, int K, int TX, int NT, int VPS, bool ZF>
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
 static int launch_fast_t(const BpArgs &a, cudaStream_t st, int *ntiles) {
-  using C = FastCfg<STORE, S, K, TX, NT, VPS, ZF>;
-  auto kern = bp_fast_kernel<STORE, S, K, TX, NT, VPS, ZF>;
+  using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
+  auto kern = bp_fast_kernel<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   size_t smem = C::smem(a.nviews);
-  if (smem > 200 * 1024) return TG_ERR_UNSUPPORTED;
+  if (smem > 220 * 1024) return TG_ERR_UNSUPPORTED;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(bp_fast)");
   dim3 grid((a.onx + TX - 1) / TX, (a.onz + C::TZ - 1) / C::TZ, (a.ny + S - 1) / S);
   if (ntiles) *ntiles = grid.x * grid.y;
-  kern<<<grid, NT, smem, st>>>(a);
+  kern<<<grid, C::NTHR, smem, st>>>(a);
   return TG_OK;
 }
 
 template <int STORE, bool ZF>
 static int launch_fast_v(const BpArgs &a, int variant, cudaStream_t st, int *ntiles) {
   switch (variant) {
-    case 0: return launch_fast_t<STORE, 8, 4, 64, 256, 4, ZF>(a, st, ntiles);
-    case 1: return launch_fast_t<STORE, 8, 8, 64, 256, 2, ZF>(a, st, ntiles);
-    case 2: return launch_fast_t<STORE, 8, 4, 32, 128, 4, ZF>(a, st, ntiles);
-    case 3: return launch_fast_t<STORE, 4, 8, 64, 256, 4, ZF>(a, st, ntiles);
-    default: return launch_fast_t<STORE, 8, 2, 128, 256, 4, ZF>(a, st, ntiles);
+    case 0: return launch_fast_t<STORE, 8, 4, 32, 128, 2, 4, ZF>(a, st, ntiles);
+    case 1: return launch_fast_t<STORE, 8, 4, 32, 128, 4, 3, ZF>(a, st, ntiles);
+    case 2: return launch_fast_t<STORE, 8, 4, 32, 256, 2, 4, ZF>(a, st, ntiles);
+    case 3: return launch_fast_t<STORE, 8, 4, 64, 256, 2, 4, ZF>(a, st, ntiles);
+    case 4: return launch_fast_t<STORE, 16, 2, 32, 128, 2, 4, ZF>(a, st, ntiles);
+    case 5: return launch_fast_t<STORE, 16, 2, 32, 256, 2, 4, ZF>(a, st, ntiles);
+    default: return launch_fast_t<STORE, 8, 8, 32, 128, 2, 4, ZF>(a, st, ntiles);
   }
 }
 

@@ -63,6 +63,23 @@ int tg_mrc_write_f32(const char *path, const uint8_t header[1024], const float *
   return TG_OK;
 }
 
+int tg_tilt_output_header(const uint8_t in_header[1024], int32_t out_nx, int32_t out_nz, uint8_t out[1024]) {
+  if (!in_header || !out) return TG_ERR_INVALID_ARG;
+  mrc::Header h = mrc::Header::from_bytes(in_header, false);
+  if (h.nx <= 0 || out_nx <= 0 || out_nz <= 0) return TG_ERR_INVALID_ARG;
+  const int out_ny = h.ny;
+  mrc::Header oh = mrc::Header::make(out_nx, out_nz, out_ny, mrc::FLOAT);
+  oh.xlen = h.xlen * (float)out_nx / (float)h.nx;
+  oh.ylen = h.xlen * (float)out_nz / (float)h.nx;
+  oh.zlen = h.ylen;
+  oh.mx = out_nx;
+  oh.my = out_nz;
+  oh.mz = out_ny;
+  oh.add_label("tilt: " + std::to_string(h.nz) + " projections, thickness " + std::to_string(out_nz));
+  oh.to_bytes(out, false);
+  return TG_OK;
+}
+
 int tg_read_tilt_file(const char *path, float *out, int32_t cap, int32_t *n) {
   if (!path || !n) return TG_ERR_INVALID_ARG;
   std::vector<float> a;

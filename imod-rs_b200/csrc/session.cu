@@ -9,6 +9,7 @@
 // computed on the host in the reference's f32 expressions, so the device
 // makes the same sampling decisions as the reference.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -306,6 +307,10 @@ static int launch_bp(tg_session *s, int mode, int *ntiles) {
 // (process-wide cache keyed by the series shape).
 static int autotune(tg_session *s) {
   if (!s->fast) { s->variant = 0; return TG_OK; }
+  if (const char *env = getenv("TG_BP_VARIANT")) {  // fixed tile shape (profiling, tuning)
+    int v = atoi(env);
+    if (v >= 0 && v < bp_fast_variants()) { s->variant = v; return TG_OK; }
+  }
   auto key = std::make_tuple(s->nx, s->onx, s->onz, s->nviews, s->store, (int)s->zf_any, s->ny >= 64 ? 64 : s->ny);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -488,7 +493,8 @@ int tg_session_create(const tg_geometry *g, const tg_options *opt, tg_session **
     int padR = needR + 6;
     s->PW = (s->padL + s->nx + padR + 1) & ~1;
   }
-  s->rows_alloc = s->fmt == FMT_ROWPAIR ? ((s->ny + 7) / 8) * 4 : s->ny;
+  const int ra = bp_fast_row_align();  // a tile's row pairs never pass the allocation
+  s->rows_alloc = s->fmt == FMT_ROWPAIR ? ((s->ny + ra - 1) / ra) * (ra / 2) : s->ny;
 
   // FFT plan or circulant fallback
   s->use_conv = !fft_plan(s->nx, &s->plan);

@@ -93,6 +93,7 @@ const char *bp_fast_variant_name(int v);
 // General kernel: x-tilt, z-factor, local alignment, SINGLE format.
 int launch_bp_general(const BpArgs &a, int store, cudaStream_t st, int *ntiles_out);
 int bp_fast_ntiles(const BpArgs &a, int variant);
+int bp_fast_row_align();  // slices per tile of the widest fast variant
 
 // ---- reprojection (main.rs:831-896) ----
 struct FpArgs {

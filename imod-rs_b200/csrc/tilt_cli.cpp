@@ -322,14 +322,10 @@ int main(int argc, char **argv) {
     tg_session_destroy(s);
     return 1;
   }
-  mrc::Header oh = mrc::Header::make(out_nx, out_nz, out_ny, mrc::FLOAT);  // main.rs:710-717
-  oh.xlen = h.xlen * (float)out_nx / (float)in_nx;
-  oh.ylen = h.xlen * (float)out_nz / (float)in_nx;
-  oh.zlen = h.ylen;
-  oh.mx = out_nx;
-  oh.my = out_nz;
-  oh.mz = out_ny;
-  oh.add_label("tilt: " + std::to_string(nz) + " projections, thickness " + std::to_string(out_nz));
+  uint8_t hin[1024], hout[1024];  // main.rs:710-717
+  h.to_bytes(hin, false);
+  tg_tilt_output_header(hin, out_nx, out_nz, hout);
+  mrc::Header oh = mrc::Header::from_bytes(hout, false);
   mrc::Writer w;
   if (!w.create(args.output, oh, &err)) {
     fprintf(stderr, "Error: %s\n", err.c_str());

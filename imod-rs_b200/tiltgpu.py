@@ -62,6 +62,13 @@ class PhantomSpec(C.Structure):
                 ("noise_kind", _i32), ("noise", _f), ("xtilt_deg", _f)]
 
 
+class MrcInfo(C.Structure):
+    _fields_ = [("nx", _i32), ("ny", _i32), ("nz", _i32), ("mode", _i32), ("next", _i32),
+                ("swapped", _i32), ("xlen", _f), ("ylen", _f), ("zlen", _f), ("amin", _f),
+                ("amax", _f), ("amean", _f), ("nlabl", _i32), ("imod", _i32),
+                ("header", C.c_uint8 * 1024)]
+
+
 class TiltGpuError(RuntimeError):
     def __init__(self, code, msg=""):
         self.code = code
@@ -94,6 +101,12 @@ EXPORTS = {
     "tg_apply_rweighting": (C.c_int, [_P, C.c_size_t, C.c_size_t, C.c_size_t, _f, _f, _i32,
                                       _i32, _i32]),
     "tg_synth_projections": (C.c_int, [C.POINTER(PhantomSpec), _P, _P, _i32, _i32]),
+    "tg_mrc_header_new": (C.c_int, [_i32, _i32, _i32, _i32, C.c_char_p, _P]),
+    "tg_mrc_read": (C.c_int, [C.c_char_p, C.POINTER(MrcInfo), _i32, _i32, _P]),
+    "tg_mrc_write_f32": (C.c_int, [C.c_char_p, _P, _P, _i32, _f, _f, _f]),
+    "tg_tilt_output_header": (C.c_int, [_P, _i32, _i32, _P]),
+    "tg_read_tilt_file": (C.c_int, [C.c_char_p, _P, _i32, C.POINTER(_i32)]),
+    "tg_write_tilt_file": (C.c_int, [C.c_char_p, _P, _i32]),
 }
 # library-internal helpers exported for tests and the benchmark (not in the header)
 EXTRA = {
@@ -331,3 +344,57 @@ def synth_projections(angles, *, nx, ny, vol_nx=None, vol_nz, n_ell=300, rmin=3.
     out = np.empty((len(ang), ny, nx), np.float32)
     check(lib().tg_synth_projections(C.byref(sp), _ptr(ang), _ptr(out), 0, device))
     return out
+
+
+# ---- MRC / tilt-file boundary (host only) ----
+MODES = {"Byte": 0, "Short": 1, "Float": 2, "ComplexShort": 3, "ComplexFloat": 4, "UShort": 6,
+         "HalfFloat": 12, "Rgb": 16, "FourBit": 101}
+
+
+def mrc_header_new(nx, ny, nz, mode, label=None) -> bytes:
+    buf = (C.c_uint8 * 1024)()
+    check(lib().tg_mrc_header_new(nx, ny, nz, MODES.get(mode, mode) if isinstance(mode, str) else mode,
+                                  None if label is None else label.encode(), buf))
+    return bytes(buf)
+
+
+def mrc_info(path):
+    info = MrcInfo()
+    check(lib().tg_mrc_read(str(path).encode(), C.byref(info), 0, 0, None))
+    return info
+
+
+def mrc_read(path, z0=0, z1=None, values_per_section=None):
+    info = mrc_info(path)
+    z1 = info.nz if z1 is None else z1
+    per = values_per_section or info.nx * info.ny * (3 if info.mode == 16 else 1)
+    out = np.empty((z1 - z0) * per, np.float32)
+    check(lib().tg_mrc_read(str(path).encode(), None, z0, z1, _ptr(out)))
+    return info, out
+
+
+def mrc_write_f32(path, header: bytes, data, stats=(0.0, 0.0, 0.0)):
+    hb = (C.c_uint8 * 1024).from_buffer_copy(header)
+    d = _f32(data)
+    nx, ny = np.frombuffer(header[:8], "<i4")
+    nsec = d.size // int(nx * ny) if d is not None else 0
+    check(lib().tg_mrc_write_f32(str(path).encode(), hb, _ptr(d), nsec, *stats))
+
+
+def tilt_output_header(in_header: bytes, out_nx, out_nz) -> bytes:
+    hin = (C.c_uint8 * 1024).from_buffer_copy(in_header)
+    out = (C.c_uint8 * 1024)()
+    check(lib().tg_tilt_output_header(hin, out_nx, out_nz, out))
+    return bytes(out)
+
+
+def read_tilt_file(path, cap=100000):
+    out = np.empty(cap, np.float32)
+    n = _i32()
+    check(lib().tg_read_tilt_file(str(path).encode(), _ptr(out), cap, C.byref(n)))
+    return out[:min(n.value, cap)].copy()
+
+
+def write_tilt_file(path, angles):
+    a = _f32(angles)
+    check(lib().tg_write_tilt_file(str(path).encode(), _ptr(a), len(a)))

@@ -210,6 +210,11 @@ int tg_mrc_read(const char *path, tg_mrc_info *info, int32_t z0, int32_t z1, flo
  * finish(amin, amax, amean).  header: 1024 little-endian bytes. */
 int tg_mrc_write_f32(const char *path, const uint8_t header[1024], const float *data,
                      int32_t nsec, float amin, float amax, float amean);
+/* Output header of a reconstruction (apps/tilt/src/main.rs:710-717): from the
+ * input stack's header bytes, the output width/thickness and the number of
+ * sections; statistics are filled in by tg_mrc_write_f32's finish. */
+int tg_tilt_output_header(const uint8_t in_header[1024], int32_t out_nx, int32_t out_nz,
+                          uint8_t out[1024]);
 /* read_tilt_file: up to cap angles into out, count in *n. */
 int tg_read_tilt_file(const char *path, float *out, int32_t cap, int32_t *n);
 /* write_tilt_file ("{:10.2}" per line). */
