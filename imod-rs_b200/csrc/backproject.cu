@@ -89,6 +89,20 @@ __device__ __forceinline__ float add_f32_bf16(float acc, uint16_t h) {
   asm("add.rn.f32.bf16 %0, %1, %2;" : "=f"(d) : "h"(h), "f"(acc));
   return d;
 }
+// acc0 += (f32)lo(h2), acc1 += (f32)hi(h2): the halves are taken straight from
+// the 32-bit register (mov.b32 unpack) instead of being shifted out
+__device__ __forceinline__ void add2_f32_f16(float &acc0, float &acc1, uint32_t h2) {
+  asm("{\n .reg .f16 lo, hi;\n mov.b32 {lo, hi}, %2;\n"
+      " add.rn.f32.f16 %0, lo, %0;\n add.rn.f32.f16 %1, hi, %1;\n}\n"
+      : "+f"(acc0), "+f"(acc1)
+      : "r"(h2));
+}
+__device__ __forceinline__ void add2_f32_bf16(float &acc0, float &acc1, uint32_t h2) {
+  asm("{\n .reg .b16 lo, hi;\n mov.b32 {lo, hi}, %2;\n"
+      " add.rn.f32.bf16 %0, lo, %0;\n add.rn.f32.bf16 %1, hi, %1;\n}\n"
+      : "+f"(acc0), "+f"(acc1)
+      : "r"(h2));
+}
 
 // Packed FP32x2 arithmetic (PTX 8.6, sm_100+): two IEEE round-to-nearest f32
 // operations per instruction, each lane identical to the scalar operation.
@@ -358,9 +372,7 @@ __global__ void __launch_bounds__(NT + 32) bp_fast_kernel(BpArgs a) {
               const uint2 e = lds64i<sp * WMAX * 8>(addr);
               const __half2 r = __hfma2(f2, *reinterpret_cast<const __half2 *>(&e.y),
                                         *reinterpret_cast<const __half2 *>(&e.x));
-              const uint32_t rb = *reinterpret_cast<const uint32_t *>(&r);
-              acc[2 * sp][j] = add_f32_f16(acc[2 * sp][j], (uint16_t)(rb & 0xffffu));
-              acc[2 * sp + 1][j] = add_f32_f16(acc[2 * sp + 1][j], (uint16_t)(rb >> 16));
+              add2_f32_f16(acc[2 * sp][j], acc[2 * sp + 1][j], *reinterpret_cast<const uint32_t *>(&r));
             });
           } else {
             const __nv_bfloat162 f2 = __float2bfloat162_rn(f0);
@@ -369,9 +381,7 @@ __global__ void __launch_bounds__(NT + 32) bp_fast_kernel(BpArgs a) {
               const uint2 e = lds64i<sp * WMAX * 8>(addr);
               const __nv_bfloat162 r = __hfma2(f2, *reinterpret_cast<const __nv_bfloat162 *>(&e.y),
                                                *reinterpret_cast<const __nv_bfloat162 *>(&e.x));
-              const uint32_t rb = *reinterpret_cast<const uint32_t *>(&r);
-              acc[2 * sp][j] = add_f32_bf16(acc[2 * sp][j], (uint16_t)(rb & 0xffffu));
-              acc[2 * sp + 1][j] = add_f32_bf16(acc[2 * sp + 1][j], (uint16_t)(rb >> 16));
+              add2_f32_bf16(acc[2 * sp][j], acc[2 * sp + 1][j], *reinterpret_cast<const uint32_t *>(&r));
             });
           }
         }

@@ -14,7 +14,7 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libtiltgpu.so")
+LIB_PATH = os.environ.get("TILTGPU_LIB") or os.path.join(_HERE, "lib", "libtiltgpu.so")
 CLI_PATH = os.path.join(_HERE, "bin", "tilt")
 
 TG_OK = 0
