@@ -9,6 +9,10 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <math.h>
+
+#include <mutex>
+
 #include "tg_internal.h"
 
 namespace tg {
@@ -326,6 +330,14 @@ __global__ void __launch_bounds__(256) filter_kernel(FilterArgs a) {
     row1 = s1;
   }
   const float fillv = a.fill ? a.fill[v] : 0.0f;
+  if (FMT == FMT_ROWS) {  // plain filtered rows written back over the input rows
+    float *o0 = reinterpret_cast<float *>(a.out) + ((size_t)v * a.ny + r0) * n;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      o0[k] = row0[k];
+      if (has1) o0[n + k] = row1[k];
+    }
+    return;
+  }
   if (FMT == FMT_ROWPAIR) {
     uint8_t *out = reinterpret_cast<uint8_t *>(a.out) +
                    ((size_t)v * a.rows_alloc + jp) * (size_t)a.PW * (STORE == TG_STORE_FP32 ? 16 : 8);
@@ -387,4 +399,115 @@ void launch_filter(const FilterArgs &a, cudaStream_t st) {
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Allocation-free R-weighting (tg_apply_rweighting_device_noalloc).
+//
+// Some callers cannot call cudaMalloc: hosts that hand every byte of device
+// memory out of their own pool or arena (a Rust or C++ host with its own
+// allocator, a framework's caching allocator), and services that must not
+// trigger cudaMalloc's implicit device-wide synchronisation or fragment device
+// memory while other streams are running.  For them this entry point filters a
+// caller-owned device stack in place and keeps its only scratch -- the
+// per-call weight, twiddle and fallback-convolution tables -- in the
+// file-scope array below, sized for rows of up to NOALLOC_MAX_NX samples.
+// Every GPU that loads this library holds the array (128 KB) until the
+// process exits.  All calls on a device share it, so calls whose GPU work
+// overlaps (on different streams, or from different host threads without
+// ordering) race on the tables; order them on one stream.
+// ---------------------------------------------------------------------------
+constexpr int NOALLOC_MAX_NX = 8192;
+// layout: weights [n] | circulant kernel [n] | twiddles [2n]
+static __device__ __align__(256) float g_rw_scratch[4 * NOALLOC_MAX_NX];
+
+static std::mutex g_rw_mu;
+static float *g_rw_dev[128];                  // device address of g_rw_scratch per device ordinal
+static float g_rw_host[4 * NOALLOC_MAX_NX];   // host staging of the tables (static, no allocation)
+
 }  // namespace tg
+
+extern "C" int tg_apply_rweighting_device_noalloc(float *dev_proj, size_t in_nx, size_t in_ny,
+                                                  size_t nz, float cutoff, float falloff,
+                                                  int32_t exact_filter_size, int32_t use_hamming,
+                                                  int32_t device, void *cuda_stream) {
+  using namespace tg;
+  if (!dev_proj || in_nx < 2 || in_ny == 0 || nz == 0) {
+    set_error("tg_apply_rweighting_device_noalloc: null pointer or empty stack");
+    return TG_ERR_INVALID_ARG;
+  }
+  if (in_nx > (size_t)NOALLOC_MAX_NX) {
+    set_error("tg_apply_rweighting_device_noalloc: rows of " + std::to_string(in_nx) +
+              " samples exceed the static scratch limit of " + std::to_string(NOALLOC_MAX_NX));
+    return TG_ERR_INVALID_ARG;
+  }
+  if ((in_ny + 1) / 2 > 65535 || nz > 65535) {
+    set_error("tg_apply_rweighting_device_noalloc: too many rows or sections for one launch");
+    return TG_ERR_INVALID_ARG;
+  }
+  if (device < 0 || device >= 128) { set_error("bad device ordinal"); return TG_ERR_INVALID_ARG; }
+  std::lock_guard<std::mutex> lk(g_rw_mu);
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  auto restore = [&]() { if (prev >= 0 && prev != device) cudaSetDevice(prev); };
+  if (!g_rw_dev[device]) {
+    // first call on this device: the array's device address (the host symbol
+    // is only a stand-in and must never be passed to a kernel)
+    void *ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_rw_scratch);
+    if (e != cudaSuccess) { restore(); return cuda_fail(e, "cudaGetSymbolAddress(g_rw_scratch)"); }
+    g_rw_dev[device] = static_cast<float *>(ptr);
+  }
+  const int n = (int)in_nx;
+  float *hw = g_rw_host, *hconv = g_rw_host + NOALLOC_MAX_NX, *htw = g_rw_host + 2 * NOALLOC_MAX_NX;
+  weight_table(n, cutoff, falloff, exact_filter_size, use_hamming, hw);
+  FilterArgs f{};
+  const bool radix = fft_plan(n, &f.plan);
+  for (int k = 0; k < n; ++k) {
+    double ang = -2.0 * M_PI * (double)k / (double)n;
+    htw[2 * k] = (float)cos(ang);
+    htw[2 * k + 1] = (float)sin(ang);
+  }
+  if (!radix)  // h[m] = (1/n) sum_k w[k] cos(2 pi k m / n)
+    for (int m = 0; m < n; ++m) {
+      double acc = 0.0;
+      for (int k = 0; k < n; ++k) acc += (double)hw[k] * cos(2.0 * M_PI * (double)k * m / n);
+      hconv[m] = (float)(acc / n);
+    }
+  float *dev = g_rw_dev[device];
+  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+  // pageable source: the copies have read the host tables when they return
+  if ((e = cudaMemcpyAsync(dev, hw, n * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (!radix && (e = cudaMemcpyAsync(dev + NOALLOC_MAX_NX, hconv, n * sizeof(float),
+                                      cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+      (e = cudaMemcpyAsync(dev + 2 * NOALLOC_MAX_NX, htw, 2 * n * sizeof(float),
+                           cudaMemcpyHostToDevice, st)) != cudaSuccess) {
+    restore();
+    return cuda_fail(e, "cudaMemcpyAsync(noalloc tables)");
+  }
+  f.in = dev_proj;
+  f.out = dev_proj;
+  f.weights = dev;
+  f.conv_h = radix ? nullptr : dev + NOALLOC_MAX_NX;
+  f.tw = reinterpret_cast<const float2 *>(dev + 2 * NOALLOC_MAX_NX);
+  f.nx = n;
+  f.ny = (int)in_ny;
+  f.nviews = (int)nz;
+  f.fill_mode = TG_FILL_ZERO;
+  f.fmt = FMT_ROWS;
+  f.store = TG_STORE_FP32;
+  f.inv_n = 1.0f / (float)n;
+  size_t smem = (size_t)n * 16;
+  auto k = filter_kernel<FMT_ROWS, TG_STORE_FP32>;
+  if (smem > 48 * 1024 &&
+      (e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) {
+    restore();
+    return cuda_fail(e, "cudaFuncSetAttribute(filter)");
+  }
+  k<<<dim3((unsigned)((in_ny + 1) / 2), (unsigned)nz), 256, smem, st>>>(f);
+  e = cudaGetLastError();
+  restore();
+  if (e != cudaSuccess) return cuda_fail(e, "filter launch (noalloc)");
+  return TG_OK;
+}

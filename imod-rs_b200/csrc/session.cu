@@ -64,7 +64,7 @@ static inline float ref_x_host(float dx, float dz, const HostView &h, float cx) 
 }
 
 // Radial weight table, apps/tilt/src/main.rs:348-369 (f32 expressions).
-static void weight_table(int n, float cutoff, float falloff, int efs, int hamming, float *wt) {
+void weight_table(int n, float cutoff, float falloff, int efs, int hamming, float *wt) {
   size_t filter_nxc = efs > 0 ? (size_t)efs : (size_t)(n / 2 + 1);
   for (int i = 0; i < n; ++i) {
     int fb = i <= n / 2 ? i : n - i;

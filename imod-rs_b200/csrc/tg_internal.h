@@ -20,7 +20,7 @@ namespace tg {
 // ([view][row-pair][PW]): FP32 float4 (a0, a1, b0, b1), FP16/BF16 uint2
 // (h2(a0,a1), h2(d0,d1)).  SINGLE keeps one row per element ([view][row][PW]):
 // FP32 float2 (a, b), FP16/BF16 uint32 h2(a, d).
-enum Fmt { FMT_ROWPAIR = 0, FMT_SINGLE = 1 };
+enum Fmt { FMT_ROWPAIR = 0, FMT_SINGLE = 1, FMT_ROWS = 2 /* plain filtered rows, in place */ };
 
 inline int elem_bytes(int fmt, int store) {
   if (fmt == FMT_ROWPAIR) return store == TG_STORE_FP32 ? 16 : 8;
@@ -62,6 +62,8 @@ struct FilterArgs {
   FftPlanDev plan;
 };
 void launch_filter(const FilterArgs &a, cudaStream_t st);
+// radial weight table of apps/tilt/src/main.rs:348-369 in f32 (host)
+void weight_table(int n, float cutoff, float falloff, int efs, int hamming, float *wt);
 
 // ---- back-projection ----
 struct LocalDev {

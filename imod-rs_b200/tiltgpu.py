@@ -101,6 +101,8 @@ EXPORTS = {
     "tg_apply_rweighting": (C.c_int, [_P, C.c_size_t, C.c_size_t, C.c_size_t, _f, _f, _i32,
                                       _i32, _i32]),
     "tg_synth_projections": (C.c_int, [C.POINTER(PhantomSpec), _P, _P, _i32, _i32]),
+    "tg_apply_rweighting_device_noalloc": (C.c_int, [_P, C.c_size_t, C.c_size_t, C.c_size_t, _f, _f,
+                                                     _i32, _i32, _i32, _P]),
     "tg_mrc_header_new": (C.c_int, [_i32, _i32, _i32, _i32, C.c_char_p, _P]),
     "tg_mrc_read": (C.c_int, [C.c_char_p, C.POINTER(MrcInfo), _i32, _i32, _P]),
     "tg_mrc_write_f32": (C.c_int, [C.c_char_p, _P, _P, _i32, _f, _f, _f]),
@@ -325,6 +327,14 @@ def apply_rweighting(proj, cutoff=0.35, falloff=0.05, exact_filter_size=None, us
     check(lib().tg_apply_rweighting(_ptr(p), nx, ny, nz, cutoff, falloff, int(exact_filter_size or 0),
                                     int(use_hamming), device))
     return p
+
+
+def apply_rweighting_device_noalloc(dev_ptr: int, nx, ny, nz, cutoff=0.35, falloff=0.05,
+                                    exact_filter_size=None, use_hamming=False, device=0, stream=0):
+    """In-place R-weighting of a device stack without any device allocation."""
+    check(lib().tg_apply_rweighting_device_noalloc(_P(dev_ptr), nx, ny, nz, cutoff, falloff,
+                                                   int(exact_filter_size or 0), int(use_hamming),
+                                                   device, _P(stream or None)))
 
 
 def synth_projections(angles, *, nx, ny, vol_nx=None, vol_nz, n_ell=300, rmin=3.0, rmax=40.0,

@@ -161,6 +161,23 @@ int tg_apply_rweighting(float *proj_data, size_t in_nx, size_t in_ny, size_t nz,
                         float falloff, int32_t exact_filter_size, int32_t use_hamming,
                         int32_t device);
 
+/* ---- Allocation-free R-weighting ----
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * hosts that hand out all device memory from their own pool or arena, and
+ * services that must avoid cudaMalloc's implicit device-wide synchronisation.
+ * Filters nz*in_ny rows of in_nx floats in place in caller-owned DEVICE memory
+ * (same arithmetic as tg_apply_rweighting), asynchronously on cuda_stream
+ * (a cudaStream_t as void*, NULL = legacy default stream).  Allocates nothing:
+ * its weight/twiddle tables live in a static 128 KB device array, which limits
+ * rows to in_nx <= 8192 (larger rows are rejected with TG_ERR_INVALID_ARG).
+ * The first call on a device looks the array up (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  All calls on a device share the
+ * array and it keeps the last call's tables: calls whose GPU work overlaps
+ * race, so order them on one stream. */
+int tg_apply_rweighting_device_noalloc(float *dev_proj, size_t in_nx, size_t in_ny, size_t nz,
+                                       float cutoff, float falloff, int32_t exact_filter_size,
+                                       int32_t use_hamming, int32_t device, void *cuda_stream);
+
 /* ---- Synthetic seeded inputs (no counterpart in the reference; the
  * workload generator for tests and benchmarks) ----
  * Projects a seeded random ellipsoid phantom (n_ell ellipsoids with semi-axes
