@@ -26,6 +26,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "tg_internal.h"
@@ -165,6 +166,7 @@ struct FastCfg {
   static constexpr int OZG = NT / TX;        // depth groups of consumer threads
   static constexpr int TZ = OZG * K;         // tile depth
   static constexpr int NTHR = NT + 32;       // consumers + one producer warp
+  static constexpr int NSTAGE_ = NSTAGE, NT_ = NT;
   static constexpr int EB = STORE == TG_STORE_FP32 ? 16 : 8;
   static constexpr int WMAX = ((TX + TZ * (ZF ? 2 : 1) + 8) + 1) & ~1;  // window elements, even
   static constexpr int SLOT = SP * WMAX * EB;                             // bytes per view
@@ -212,21 +214,39 @@ __device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t parity, volati
 // per-view row windows with cp.async.bulk, one copy per lane, completing on
 // full[b]; consumer warps wait on full[b], accumulate, and release the buffer
 // on empty[b].  NSTAGE buffers of VPS views form a ring.
+// Shared-memory layout of a CTA: the stage ring, the per-view windows (sized
+// for max_views) and the 2*NSTAGE mbarriers.
+template <class C> struct SmemLayout {
+  unsigned char *bufs;
+  int *win_k0, *win_n;
+  uint64_t *full, *empty;
+  __device__ SmemLayout(unsigned char *sm, int max_views) {
+    bufs = sm;
+    win_k0 = reinterpret_cast<int *>(sm + C::BUF);
+    win_n = win_k0 + max_views;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(
+        (reinterpret_cast<uintptr_t>(win_n + max_views) + 15) & ~(uintptr_t)15);
+    full = bars;
+    empty = bars + C::NSTAGE_;
+  }
+};
+
+// One output tile (S slices x TX columns x TZ depths) of one series.  gst is the
+// CTA's running stage count: ring slots and mbarrier phases continue across the
+// tiles a persistent CTA processes.  Returns false on abort.
 template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
-__global__ void __launch_bounds__(NT + 32) bp_fast_kernel(BpArgs a) {
+__device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz, unsigned char *sm,
+                                        const SmemLayout<FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>> &L,
+                                        int &gst, volatile int *s_abort_p) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   constexpr int SP = C::SP, OZG = C::OZG, TZ = C::TZ, EB = C::EB, WMAX = C::WMAX, SLOT = C::SLOT;
-  extern __shared__ __align__(128) unsigned char sm[];
-  unsigned char *bufs = sm;
-  int *win_k0 = reinterpret_cast<int *>(sm + C::BUF);
-  int *win_n = win_k0 + a.nviews;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(
-      (reinterpret_cast<uintptr_t>(win_n + a.nviews) + 15) & ~(uintptr_t)15);
-  uint64_t *full = bars, *empty = bars + NSTAGE;
-  __shared__ volatile int s_abort;
+  unsigned char *bufs = L.bufs;
+  int *win_k0 = L.win_k0, *win_n = L.win_n;
+  uint64_t *full = L.full, *empty = L.empty;
+  volatile int &s_abort = *s_abort_p;
 
   const int tid = threadIdx.x;
-  const int ox0 = blockIdx.x * TX, oz0 = blockIdx.y * TZ, iy0 = blockIdx.z * S;
+  const int ox0 = bx * TX, oz0 = by * TZ, iy0 = bz * S;
   const int oxlo = ox0, oxhi = min(ox0 + TX, a.onx) - 1;
   const int ozlo = oz0, ozhi = min(oz0 + TZ, a.onz) - 1;
 
@@ -254,30 +274,23 @@ __global__ void __launch_bounds__(NT + 32) bp_fast_kernel(BpArgs a) {
     win_k0[v] = kmin;
     win_n[v] = cnt;
   }
-  if (tid == 0) {
-    for (int b = 0; b < NSTAGE; ++b) {
-      mbar_init(smem_u32(&full[b]), 1);
-      mbar_init(smem_u32(&empty[b]), NT / 32);
-    }
-    fence_mbar_init();
-    s_abort = 0;
-  }
   __syncthreads();
 
   const int nst = (a.nviews + VPS - 1) / VPS;
+  const int g0 = gst;  // global index of this tile's first stage
+  gst += nst;
   if (tid >= NT) {
     // ---------------- producer warp ----------------
     const int lane = tid - NT;
     const uint8_t *pairs = reinterpret_cast<const uint8_t *>(a.pairs);
     const int jp0 = iy0 / 2;
-    int issued = 0;
     for (int st = 0; st < nst; ++st) {
-      const int b = st % NSTAGE;
-      if (st >= NSTAGE && !wait_phase(smem_u32(&empty[b]), ((st / NSTAGE) - 1) & 1, &s_abort)) {
+      const int g = g0 + st, b = g % NSTAGE;
+      if (g >= NSTAGE && !wait_phase(smem_u32(&empty[b]), ((g / NSTAGE) - 1) & 1, &s_abort)) {
         s_abort = 1;
-        break;
+        return false;
       }
-      if (s_abort) break;
+      if (s_abort) return false;
       const int v0 = st * VPS, nv = min(VPS, a.nviews - v0);
       const bool mine = lane < nv * SP;
       const int vi = lane / SP, sp = lane % SP, v = v0 + vi;
@@ -294,13 +307,8 @@ __global__ void __launch_bounds__(NT + 32) bp_fast_kernel(BpArgs a) {
         const uint32_t dst = smem_u32(bufs) + (b * VPS + vi) * SLOT + sp * WMAX * EB;
         bulk_g2s(dst, src, bytes, smem_u32(&full[b]));
       }
-      ++issued;
     }
-    // no copy may still be landing when the CTA exits: bounded wait on the last stages
-    if (lane == 0)
-      for (int st = max(0, issued - NSTAGE); st < issued; ++st)
-        wait_phase(smem_u32(&full[st % NSTAGE]), (st / NSTAGE) & 1, &s_abort);
-    return;
+    return true;
   }
 
   // ---------------- consumer warps ----------------
@@ -326,8 +334,8 @@ __global__ void __launch_bounds__(NT + 32) bp_fast_kernel(BpArgs a) {
 
   bool ok = true;
   for (int st = 0; st < nst && ok; ++st) {
-    const int b = st % NSTAGE;
-    if (!wait_phase(smem_u32(&full[b]), (st / NSTAGE) & 1, &s_abort)) {
+    const int g = g0 + st, b = g % NSTAGE;
+    if (!wait_phase(smem_u32(&full[b]), (g / NSTAGE) & 1, &s_abort)) {
       s_abort = 1;
       ok = false;
       break;
@@ -393,14 +401,14 @@ __global__ void __launch_bounds__(NT + 32) bp_fast_kernel(BpArgs a) {
   consumer_sync(NT);  // all consumers past the loop (buffers free, abort flag settled)
   if (s_abort) {
     if (tid == 0) atomicOr(a.err, 1);
-    return;
+    return false;
   }
 
   // ---- epilogue: 1/N, output transform or SIRT update, per-slice partial stats
   const int oxr = ox0 + tx;
   const bool xok = oxr < a.onx;
   float *red = reinterpret_cast<float *>(sm);  // staging buffers are free now
-  const int tile = blockIdx.x + blockIdx.y * gridDim.x;
+  const int tile = bx + by * a.nbx;
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     const int iy = iy0 + s;
@@ -461,10 +469,81 @@ __global__ void __launch_bounds__(NT + 32) bp_fast_kernel(BpArgs a) {
       p.mn = mn;
       p.mx = mx;
       p.sum = sum;
-      a.partial[(size_t)(iy0 + tid) * (gridDim.x * gridDim.y) + tile] = p;
+      a.partial[(size_t)(iy0 + tid) * a.ntiles_xz + tile] = p;
     }
   }
+  return true;
 }
+
+template <class C> __device__ __forceinline__ void init_ring(const SmemLayout<C> &L, volatile int *s_abort) {
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < C::NSTAGE_; ++b) {
+      mbar_init(smem_u32(&L.full[b]), 1);
+      mbar_init(smem_u32(&L.empty[b]), C::NT_ / 32);
+    }
+    fence_mbar_init();
+    *s_abort = 0;
+  }
+}
+
+// The producer leaves no copy landing in shared memory after the CTA exits
+// (only possible after an abort): bounded wait on the last NSTAGE stages.
+template <class C> __device__ __forceinline__ void drain_ring(const SmemLayout<C> &L, int gst,
+                                                              volatile int *s_abort) {
+  if (threadIdx.x == C::NT_ && *s_abort)
+    for (int g = max(0, gst - C::NSTAGE_); g < gst; ++g)
+      wait_phase(smem_u32(&L.full[g % C::NSTAGE_]), (g / C::NSTAGE_) & 1, s_abort);
+}
+
+// One launch per series: grid = tiles of that series.
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
+__global__ void __launch_bounds__(NT + 32) bp_fast_kernel(const __grid_constant__ BpArgs a) {
+  using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
+  extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ volatile int s_abort;
+  const SmemLayout<C> L(sm, a.nviews);
+  init_ring(L, &s_abort);
+  int gst = 0;
+  bp_tile<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>(a, blockIdx.x, blockIdx.y, blockIdx.z, sm, L, gst, &s_abort);
+  drain_ring(L, gst, &s_abort);
+}
+
+// Persistent launch over the tiles of many series: each CTA takes the next
+// tile of the queue (longest series first) until it is empty.  Each tile's
+// arithmetic is the same as in the per-series kernel, so every series' result
+// does not depend on what else is in the batch.
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
+__global__ void __launch_bounds__(NT + 32) bp_batch_kernel(const BpArgs *__restrict__ jobs,
+                                                           const int4 *__restrict__ tiles, int ntiles,
+                                                           int *counter, int max_views) {
+  using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
+  extern __shared__ __align__(128) unsigned char sm[];
+  __shared__ volatile int s_abort;
+  __shared__ int s_tile;
+  __shared__ __align__(16) BpArgs s_args;
+  const SmemLayout<C> L(sm, max_views);
+  init_ring(L, &s_abort);
+  int gst = 0;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
+    __syncthreads();
+    const int t = s_tile;
+    if (t >= ntiles || s_abort) break;
+    const int4 T = tiles[t];  // (job, bx, by, bz)
+    {
+      const uint32_t *src = reinterpret_cast<const uint32_t *>(&jobs[T.x]);
+      uint32_t *dst = reinterpret_cast<uint32_t *>(const_cast<BpArgs *>(&s_args));
+      for (int i = threadIdx.x; i < (int)(sizeof(BpArgs) / 4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    if (!bp_tile<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>(s_args, T.y, T.z, T.w, sm, L, gst, &s_abort)) {
+      s_abort = 1;
+    }
+  }
+  drain_ring(L, gst, &s_abort);
+}
+
+
 
 // ---- variant table (tile shapes the autotuner chooses from) ----
 struct FastVariant { int S, K, TX, NT, VPS, NSTAGE; const char *name; };
@@ -483,16 +562,39 @@ const char *bp_fast_variant_name(int v) { return kFast[v].name; }
 int bp_fast_row_align() { return MAX_S; }
 
 template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
-static int launch_fast_t(const BpArgs &a, cudaStream_t st, int *ntiles) {
+static int launch_fast_t(const BpArgs &a0, cudaStream_t st, int *ntiles) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   auto kern = bp_fast_kernel<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
-  size_t smem = C::smem(a.nviews);
+  size_t smem = C::smem(a0.nviews);
   if (smem > 220 * 1024) return TG_ERR_UNSUPPORTED;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(bp_fast)");
-  dim3 grid((a.onx + TX - 1) / TX, (a.onz + C::TZ - 1) / C::TZ, (a.ny + S - 1) / S);
+  dim3 grid((a0.onx + TX - 1) / TX, (a0.onz + C::TZ - 1) / C::TZ, (a0.ny + S - 1) / S);
+  BpArgs a = a0;
+  a.nbx = grid.x;
+  a.ntiles_xz = grid.x * grid.y;
   if (ntiles) *ntiles = grid.x * grid.y;
   kern<<<grid, C::NTHR, smem, st>>>(a);
+  return TG_OK;
+}
+
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
+static int launch_batch_t(const BatchLaunch &bl, cudaStream_t st) {
+  using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
+  auto kern = bp_batch_kernel<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
+  size_t smem = C::smem(bl.max_views);
+  if (smem > 220 * 1024) return TG_ERR_UNSUPPORTED;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(bp_batch)");
+  int dev = 0, nsm = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::NTHR, smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  const int grid = std::max(1, std::min(bl.ntiles, nsm * std::max(1, per_sm)));
+  e = cudaMemsetAsync(bl.counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(tile counter)");
+  kern<<<grid, C::NTHR, smem, st>>>(bl.jobs, bl.tiles, bl.ntiles, bl.counter, bl.max_views);
   return TG_OK;
 }
 
@@ -507,6 +609,35 @@ static int launch_fast_v(const BpArgs &a, int variant, cudaStream_t st, int *nti
     case 5: return launch_fast_t<STORE, 16, 2, 32, 256, 2, 4, ZF>(a, st, ntiles);
     default: return launch_fast_t<STORE, 8, 8, 32, 128, 2, 4, ZF>(a, st, ntiles);
   }
+}
+
+template <int STORE, bool ZF>
+static int launch_batch_v(const BatchLaunch &bl, int variant, cudaStream_t st) {
+  switch (variant) {
+    case 0: return launch_batch_t<STORE, 8, 4, 32, 128, 2, 4, ZF>(bl, st);
+    case 1: return launch_batch_t<STORE, 8, 4, 32, 128, 4, 3, ZF>(bl, st);
+    case 2: return launch_batch_t<STORE, 8, 4, 32, 256, 2, 4, ZF>(bl, st);
+    case 3: return launch_batch_t<STORE, 8, 4, 64, 256, 2, 4, ZF>(bl, st);
+    case 4: return launch_batch_t<STORE, 16, 2, 32, 128, 2, 4, ZF>(bl, st);
+    case 5: return launch_batch_t<STORE, 16, 2, 32, 256, 2, 4, ZF>(bl, st);
+    default: return launch_batch_t<STORE, 8, 8, 32, 128, 2, 4, ZF>(bl, st);
+  }
+}
+
+int launch_bp_batch(const BatchLaunch &bl, int store, bool zf, int variant, cudaStream_t st) {
+  if (variant < 0 || variant >= bp_fast_variants()) variant = 0;
+  if (store == TG_STORE_FP32)
+    return zf ? launch_batch_v<TG_STORE_FP32, true>(bl, variant, st) : launch_batch_v<TG_STORE_FP32, false>(bl, variant, st);
+  if (store == TG_STORE_FP16)
+    return zf ? launch_batch_v<TG_STORE_FP16, true>(bl, variant, st) : launch_batch_v<TG_STORE_FP16, false>(bl, variant, st);
+  return zf ? launch_batch_v<TG_STORE_BF16, true>(bl, variant, st) : launch_batch_v<TG_STORE_BF16, false>(bl, variant, st);
+}
+
+void bp_fast_tile_shape(int variant, int *S, int *TX, int *TZ) {
+  const FastVariant &f = kFast[variant < 0 || variant >= bp_fast_variants() ? 0 : variant];
+  *S = f.S;
+  *TX = f.TX;
+  *TZ = (f.NT / f.TX) * f.K;
 }
 
 int bp_fast_ntiles(const BpArgs &a, int variant) {

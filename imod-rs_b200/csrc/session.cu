@@ -21,7 +21,7 @@
 #include <tuple>
 #include <vector>
 
-#include "tg_internal.h"
+#include "session_impl.h"
 
 namespace tg {
 
@@ -107,37 +107,6 @@ static std::map<std::tuple<int, int, int, int, int, int, int>, int> g_tune;
 }  // namespace tg
 
 using namespace tg;
-
-struct tg_session {
-  int nx = 0, ny = 0, nz = 0, onx = 0, onz = 0, nviews = 0;
-  tg_options o{};
-  bool has_local = false, fast = true, zf_any = false;
-  int fmt = FMT_ROWPAIR, store = TG_STORE_FP32;
-  int padL = 0, PW = 0, rows_alloc = 0, variant = -1, ntiles_cap = 0;
-  int dev = 0;
-  cudaStream_t st = nullptr, own_st = nullptr;
-  float *d_raw = nullptr, *d_means = nullptr, *d_vol = nullptr, *d_sino = nullptr, *d_tmp = nullptr;
-  double *d_mpart = nullptr;
-  void *d_pairs = nullptr;
-  size_t pairs_bytes = 0;
-  StatPartial *d_part = nullptr;
-  float *d_slice_stats = nullptr, *d_stats3 = nullptr;
-  float4 *d_vg = nullptr, *d_vg2 = nullptr;
-  float *d_weights = nullptr, *d_conv = nullptr, *d_stretch = nullptr;
-  float2 *d_tw = nullptr;
-  int *d_err = nullptr;
-  int4 *d_lvinfo = nullptr;
-  int *d_lgoff = nullptr;
-  float *d_lxs = nullptr, *d_lys = nullptr, *d_lgdx = nullptr, *d_lgdy = nullptr;
-  FftPlanDev plan{};
-  bool use_conv = false;
-  bool uploaded = false, prepared = false;
-  size_t dev_bytes = 0;
-  tg_run_info info{};
-  cudaEvent_t ev[6] = {};
-  cudaGraphExec_t sirt_exec = nullptr;
-  float cx = 0, cz = 0, ocx = 0, inv_n = 0;
-};
 
 namespace tg {
 
@@ -231,7 +200,7 @@ static int upload_local(tg_session *s, const float *rows, int nrows, std::vector
   return TG_OK;
 }
 
-static LocalDev local_dev(tg_session *s) {
+LocalDev local_dev(tg_session *s) {
   LocalDev L{};
   L.vinfo = s->d_lvinfo;
   L.goff = s->d_lgoff;
@@ -242,7 +211,7 @@ static LocalDev local_dev(tg_session *s) {
   return L;
 }
 
-static BpArgs bp_args(tg_session *s, int mode) {
+BpArgs bp_args(tg_session *s, int mode) {
   BpArgs a{};
   a.pairs = s->d_pairs;
   a.vg = s->d_vg;
@@ -272,7 +241,7 @@ static BpArgs bp_args(tg_session *s, int mode) {
   return a;
 }
 
-static FilterArgs filter_args(tg_session *s, bool residual) {
+FilterArgs filter_args(tg_session *s, bool residual) {
   FilterArgs f{};
   f.in = s->d_raw;
   f.sub = residual ? s->d_sino : nullptr;
@@ -297,7 +266,7 @@ static FilterArgs filter_args(tg_session *s, bool residual) {
   return f;
 }
 
-static int launch_bp(tg_session *s, int mode, int *ntiles) {
+int launch_bp(tg_session *s, int mode, int *ntiles) {
   BpArgs a = bp_args(s, mode);
   if (s->fast) return launch_bp_fast(a, s->store, s->zf_any, s->variant < 0 ? 0 : s->variant, s->st, ntiles);
   return launch_bp_general(a, s->store, s->st, ntiles);
@@ -305,7 +274,7 @@ static int launch_bp(tg_session *s, int mode, int *ntiles) {
 
 // Times each fast tile variant once on this series and keeps the fastest
 // (process-wide cache keyed by the series shape).
-static int autotune(tg_session *s) {
+int autotune(tg_session *s) {
   if (!s->fast) { s->variant = 0; return TG_OK; }
   if (const char *env = getenv("TG_BP_VARIANT")) {  // fixed tile shape (profiling, tuning)
     int v = atoi(env);
@@ -341,6 +310,54 @@ static int autotune(tg_session *s) {
   s->variant = best;
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[key] = best;
+  return TG_OK;
+}
+
+FpArgs fp_args(tg_session *s) {
+  FpArgs f{};
+  f.vol = s->d_vol;
+  f.sino = s->d_sino;
+  f.vg = s->d_vg;
+  f.vg2 = s->d_vg2;
+  f.nx = s->nx;
+  f.ny = s->ny;
+  f.nviews = s->nviews;
+  f.nviews_all = s->nviews;
+  f.onx = s->onx;
+  f.onz = s->onz;
+  f.cx = s->cx;
+  f.cz = s->cz;
+  f.ocx = s->ocx;
+  f.has_local = s->has_local;
+  f.loc = local_dev(s);
+  return f;
+}
+
+int stage_front(tg_session *s, int *launches) {
+  if (!s->prepared) {
+    launch_log_means(s->d_raw, s->nx * s->ny, s->nz, s->o.log_transform, s->d_mpart, s->d_means, s->st);
+    *launches += 2;
+    s->prepared = true;
+  }
+  launch_filter(filter_args(s, false), s->st);
+  *launches += 1;
+  TG_CUDA(cudaGetLastError());
+  return TG_OK;
+}
+
+int stage_finish(tg_session *s, int mode0, int ntiles, int *launches) {
+  for (int k = 0; k < fake_passes(s); ++k) {
+    launch_lowpass(s->d_vol, s->d_tmp, s->onx, s->onz, s->ny, s->st);
+    *launches += 3;
+  }
+  if (mode0 == 1) {
+    launch_transform_stats(s->d_vol, s->onx, s->onz, s->ny, s->o.densweight, s->o.outscale, s->o.outadd,
+                           s->d_part, &ntiles, s->st);
+    *launches += 1;
+  }
+  launch_stats_reduce(s->d_part, s->ny, ntiles, s->onx * s->onz, s->d_slice_stats, s->d_stats3, s->st);
+  *launches += 1;
+  TG_CUDA(cudaGetLastError());
   return TG_OK;
 }
 
@@ -592,38 +609,22 @@ int tg_reconstruct(tg_session *s) {
   if (!s) return TG_ERR_INVALID_ARG;
   if (!s->uploaded) { set_error("no projections uploaded"); return TG_ERR_INVALID_ARG; }
   TG_CUDA(cudaSetDevice(s->dev));
+  (void)cudaGetLastError();  // a stale error of an earlier, unrelated call must not fail this run
   int rc, launches = 0, ntiles = 0;
   if (s->variant < 0 && (rc = autotune(s)) != TG_OK) return rc;
-  const bool compat = s->o.gpu_compat != 0;
-  const int iters = compat ? 0 : s->o.sirt_iters;
-  const int fake = compat ? 0 : s->o.fake_sirt;
+  const int iters = sirt_iters(s);
+  s->timed = false;
   TG_CUDA(cudaEventRecord(s->ev[0], s->st));
-  if (!s->prepared) {
-    launch_log_means(s->d_raw, s->nx * s->ny, s->nz, s->o.log_transform, s->d_mpart, s->d_means, s->st);
-    launches += 2;
-    s->prepared = true;
-  }
-  launch_filter(filter_args(s, false), s->st);
-  launches++;
-  TG_CUDA(cudaGetLastError());
+  if ((rc = stage_front(s, &launches)) != TG_OK) return rc;
   TG_CUDA(cudaEventRecord(s->ev[1], s->st));
-  const int mode0 = (iters > 0 || fake > 0) ? 1 : 0;
+  const int mode0 = first_mode(s);
   if ((rc = launch_bp(s, mode0, &ntiles)) != TG_OK) return rc;
   launches++;
   TG_CUDA(cudaGetLastError());
   TG_CUDA(cudaEventRecord(s->ev[2], s->st));
   if (iters > 0) {
     auto one_iter = [&]() -> int {
-      FpArgs f{};
-      f.vol = s->d_vol;
-      f.sino = s->d_sino;
-      f.vg = s->d_vg;
-      f.vg2 = s->d_vg2;
-      f.nx = s->nx; f.ny = s->ny; f.nviews = s->nviews; f.nviews_all = s->nviews;
-      f.onx = s->onx; f.onz = s->onz; f.cx = s->cx; f.cz = s->cz; f.ocx = s->ocx;
-      f.has_local = s->has_local;
-      f.loc = local_dev(s);
-      launch_reproject(f, s->st);
+      launch_reproject(fp_args(s), s->st);
       launch_filter(filter_args(s, true), s->st);
       return launch_bp(s, 2, nullptr);
     };
@@ -647,23 +648,13 @@ int tg_reconstruct(tg_session *s) {
     launches += 3 * iters;
   }
   TG_CUDA(cudaEventRecord(s->ev[3], s->st));
-  for (int k = 0; k < fake; ++k) {
-    launch_lowpass(s->d_vol, s->d_tmp, s->onx, s->onz, s->ny, s->st);
-    launches += 3;
-  }
-  if (mode0 == 1) {
-    launch_transform_stats(s->d_vol, s->onx, s->onz, s->ny, s->o.densweight, s->o.outscale, s->o.outadd,
-                           s->d_part, &ntiles, s->st);
-    launches++;
-  }
-  launch_stats_reduce(s->d_part, s->ny, ntiles, s->onx * s->onz, s->d_slice_stats, s->d_stats3, s->st);
-  launches++;
-  TG_CUDA(cudaGetLastError());
+  if ((rc = stage_finish(s, mode0, ntiles, &launches)) != TG_OK) return rc;
   TG_CUDA(cudaEventRecord(s->ev[4], s->st));
   s->info = tg_run_info{};
   s->info.passes = 1 + iters;
   s->info.updates = (double)s->onx * s->onz * s->ny * s->nviews * (1.0 + 2.0 * iters);
   s->info.kernel_launches = launches;
+  s->timed = true;
   return TG_OK;
 }
 
@@ -679,15 +670,17 @@ int tg_synchronize(tg_session *s) {
     set_error("staging window outside the padded row (internal error)");
     return TG_ERR_CUDA;
   }
-  float t[5] = {0, 0, 0, 0, 0};
-  cudaEventElapsedTime(&t[0], s->ev[0], s->ev[4]);
-  cudaEventElapsedTime(&t[1], s->ev[0], s->ev[1]);
-  cudaEventElapsedTime(&t[2], s->ev[1], s->ev[2]);
-  cudaEventElapsedTime(&t[3], s->ev[2], s->ev[3]);
-  s->info.ms_total = t[0];
-  s->info.ms_filter = t[1];
-  s->info.ms_backproject = t[2];
-  s->info.ms_reproject = t[3];
+  if (s->timed) {  // stage times of the last tg_reconstruct (not recorded for batched runs)
+    float t[4] = {0, 0, 0, 0};
+    TG_CUDA(cudaEventElapsedTime(&t[0], s->ev[0], s->ev[4]));
+    TG_CUDA(cudaEventElapsedTime(&t[1], s->ev[0], s->ev[1]));
+    TG_CUDA(cudaEventElapsedTime(&t[2], s->ev[1], s->ev[2]));
+    TG_CUDA(cudaEventElapsedTime(&t[3], s->ev[2], s->ev[3]));
+    s->info.ms_total = t[0];
+    s->info.ms_filter = t[1];
+    s->info.ms_backproject = t[2];
+    s->info.ms_reproject = t[3];
+  }
   return TG_OK;
 }
 

@@ -1,0 +1,61 @@
+// session_impl.h -- the session object and the stage helpers shared by the
+// per-series C ABI (session.cu) and the batched launch (batch.cu).
+#pragma once
+#include <vector>
+
+#include "tg_internal.h"
+
+using tg::StatPartial;
+using tg::FftPlanDev;
+using tg::FMT_ROWPAIR;
+
+struct tg_session {  // one tilt series resident on a device
+  int nx = 0, ny = 0, nz = 0, onx = 0, onz = 0, nviews = 0;
+  tg_options o{};
+  bool has_local = false, fast = true, zf_any = false;
+  int fmt = FMT_ROWPAIR, store = TG_STORE_FP32;
+  int padL = 0, PW = 0, rows_alloc = 0, variant = -1, ntiles_cap = 0;
+  int dev = 0;
+  cudaStream_t st = nullptr, own_st = nullptr;
+  float *d_raw = nullptr, *d_means = nullptr, *d_vol = nullptr, *d_sino = nullptr, *d_tmp = nullptr;
+  double *d_mpart = nullptr;
+  void *d_pairs = nullptr;
+  size_t pairs_bytes = 0;
+  StatPartial *d_part = nullptr;
+  float *d_slice_stats = nullptr, *d_stats3 = nullptr;
+  float4 *d_vg = nullptr, *d_vg2 = nullptr;
+  float *d_weights = nullptr, *d_conv = nullptr, *d_stretch = nullptr;
+  float2 *d_tw = nullptr;
+  int *d_err = nullptr;
+  int4 *d_lvinfo = nullptr;
+  int *d_lgoff = nullptr;
+  float *d_lxs = nullptr, *d_lys = nullptr, *d_lgdx = nullptr, *d_lgdy = nullptr;
+  FftPlanDev plan{};
+  bool use_conv = false;
+  bool uploaded = false, prepared = false;
+  bool timed = false;  // ev[] were recorded by the last tg_reconstruct
+  size_t dev_bytes = 0;
+  tg_run_info info{};
+  cudaEvent_t ev[6] = {};
+  cudaGraphExec_t sirt_exec = nullptr;
+  float cx = 0, cz = 0, ocx = 0, inv_n = 0;
+};
+
+namespace tg {
+
+LocalDev local_dev(tg_session *s);
+BpArgs bp_args(tg_session *s, int mode);
+FilterArgs filter_args(tg_session *s, bool residual);
+FpArgs fp_args(tg_session *s);
+int launch_bp(tg_session *s, int mode, int *ntiles);
+int autotune(tg_session *s);
+// log10 + means on first use, then the filter stage of the WBP pass
+int stage_front(tg_session *s, int *launches);
+// fake-SIRT passes, output transform (when the volume was stored raw) and statistics;
+// bp_ntiles: partial-stat tiles written by the back-projection in mode 0
+int stage_finish(tg_session *s, int mode0, int bp_ntiles, int *launches);
+inline int sirt_iters(const tg_session *s) { return s->o.gpu_compat ? 0 : s->o.sirt_iters; }
+inline int fake_passes(const tg_session *s) { return s->o.gpu_compat ? 0 : s->o.fake_sirt; }
+inline int first_mode(const tg_session *s) { return (sirt_iters(s) > 0 || fake_passes(s) > 0) ? 1 : 0; }
+
+}  // namespace tg

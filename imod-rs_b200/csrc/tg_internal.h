@@ -85,7 +85,18 @@ struct BpArgs {
   int mode;                 // 0: final (transform + stats), 1: store acc/N, 2: vol += relax*acc/N
   int has_local;
   LocalDev loc;
+  int nbx, ntiles_xz;       // tile grid of the fast kernel (set by its launcher)
 };
+// A persistent back-projection launch over the tiles of several series.
+struct BatchLaunch {
+  const BpArgs *jobs;       // device array of per-series arguments (nbx, ntiles_xz filled)
+  const int4 *tiles;        // device array of (job, bx, by, bz), longest series first
+  int ntiles;
+  int *counter;             // device int, reset by the launcher
+  int max_views;
+};
+int launch_bp_batch(const BatchLaunch &bl, int store, bool zf, int variant, cudaStream_t st);
+void bp_fast_tile_shape(int variant, int *S, int *TX, int *TZ);
 struct BpTile { int S, K, TX, NT, VPS, wmax; };
 // Fast kernel: no x-tilt, no local alignment, ROWPAIR format.
 int launch_bp_fast(const BpArgs &a, int store, bool zf, int variant, cudaStream_t st,
@@ -125,10 +136,12 @@ int synth_projections(const tg_phantom_spec *spec, const float *angles, float *d
 // ---- errors ----
 void set_error(const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
-#define TG_CUDA(call)                                         \
-  do {                                                        \
-    cudaError_t _e = (call);                                  \
-    if (_e != cudaSuccess) return ::tg::cuda_fail(_e, #call); \
+#define TG_STR2(x) #x
+#define TG_STR(x) TG_STR2(x)
+#define TG_CUDA(call)                                                                       \
+  do {                                                                                      \
+    cudaError_t _e = (call);                                                                \
+    if (_e != cudaSuccess) return ::tg::cuda_fail(_e, #call " at " __FILE__ ":" TG_STR(__LINE__)); \
   } while (0)
 
 }  // namespace tg

@@ -94,6 +94,13 @@ EXPORTS = {
     "tg_session_device_bytes": (C.c_size_t, [_P]),
     "tg_session_destroy": (C.c_int, [_P]),
     "tg_session_set_stream": (C.c_int, [_P, _P]),
+    "tg_batch_create": (C.c_int, [_i32, C.POINTER(_P)]),
+    "tg_batch_add": (C.c_int, [_P, _P]),
+    "tg_batch_clear": (C.c_int, [_P]),
+    "tg_batch_reconstruct": (C.c_int, [_P]),
+    "tg_batch_synchronize": (C.c_int, [_P]),
+    "tg_batch_last_run": (C.c_int, [_P, C.POINTER(RunInfo)]),
+    "tg_batch_destroy": (C.c_int, [_P]),
     "tg_gpu_session_new": (C.c_int, [_P, _P, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t,
                                      C.c_size_t, _i32, C.POINTER(_P)]),
     "tg_gpu_session_reconstruct_row": (C.c_int, [_P, C.c_size_t, _P]),
@@ -280,6 +287,48 @@ class Session:
 
     def __exit__(self, *a):
         self.close()
+
+
+class Batch:
+    """Many sessions reconstructed together (tg_batch_*): one persistent
+    back-projection launch per round across all fast-path series."""
+
+    def __init__(self, device=0):
+        self.h = _P()
+        check(lib().tg_batch_create(device, C.byref(self.h)))
+        self.sessions = []
+
+    def add(self, s: "Session"):
+        check(lib().tg_batch_add(self.h, s.h))
+        self.sessions.append(s)
+
+    def clear(self):
+        check(lib().tg_batch_clear(self.h))
+        self.sessions = []
+
+    def reconstruct(self, sync=True):
+        check(lib().tg_batch_reconstruct(self.h))
+        if sync:
+            self.synchronize()
+
+    def synchronize(self):
+        check(lib().tg_batch_synchronize(self.h))
+
+    def last_run(self):
+        ri = RunInfo()
+        check(lib().tg_batch_last_run(self.h, C.byref(ri)))
+        return {k: getattr(ri, k) for k, _ in RunInfo._fields_}
+
+    def close(self):
+        if self.h:
+            lib().tg_batch_destroy(self.h)
+            self.h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def reconstruct(proj, angles, **kw):

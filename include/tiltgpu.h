@@ -140,6 +140,24 @@ size_t tg_session_device_bytes(tg_session *s);
 int tg_session_set_stream(tg_session *s, void *cuda_stream);
 int tg_session_destroy(tg_session *s);
 
+/* ---- Batched reconstruction of many series (no counterpart in the reference,
+ * which reconstructs one series per process) ----
+ * Sessions (already holding their projections, all on the batch's device) are
+ * added to a batch; tg_batch_reconstruct runs every series' whole path.  The
+ * back-projection passes of all series that take the fast kernel and share a
+ * staging precision run as one persistent launch per round (round 0: WBP,
+ * round r: r-th SIRT update), with a longest-first tile queue.  Each series'
+ * result is identical to tg_reconstruct on that session alone.  Call
+ * tg_batch_synchronize before reading a session's results. */
+typedef struct tg_batch tg_batch;
+int tg_batch_create(int32_t device, tg_batch **out);
+int tg_batch_add(tg_batch *b, tg_session *s);
+int tg_batch_clear(tg_batch *b);
+int tg_batch_reconstruct(tg_batch *b);
+int tg_batch_synchronize(tg_batch *b);
+int tg_batch_last_run(tg_batch *b, tg_run_info *info);
+int tg_batch_destroy(tg_batch *b);
+
 /* ---- The reference's GPU seam, same arguments and meaning ----
  * GpuSession::new(projections, tilt_cos_sin, in_nx, in_ny, n_projs, out_nx, out_nz)
  * (apps/tilt/src/gpu.rs:43-51): projections are already filtered/stretched,
