@@ -356,7 +356,7 @@ int stage_finish(tg_session *s, int mode0, int ntiles, int *launches) {
     *launches += 1;
   }
   launch_stats_reduce(s->d_part, s->ny, ntiles, s->onx * s->onz, s->d_slice_stats, s->d_stats3, s->st);
-  *launches += 1;
+  *launches += 2;
   TG_CUDA(cudaGetLastError());
   return TG_OK;
 }

@@ -95,42 +95,61 @@ void launch_transform_stats(float *vol, int onx, int onz, int ny, float dw, floa
   if (ntiles_out) *ntiles_out = TS_TILES;
 }
 
-// One thread per slice: (min, max, f32 mean) of the slice; then thread 0 folds
-// the slices in Y order exactly as main.rs:1080-1092 does.
-__global__ void stats_reduce_kernel(const StatPartial *partial, int ny, int ntiles, int count,
-                                    float *slice_stats, float *out3) {
-  for (int iy = threadIdx.x; iy < ny; iy += blockDim.x) {
-    float mn = 3.40282347e+38f, mx = -3.40282347e+38f;
-    double sum = 0.0;
-    for (int t = 0; t < ntiles; ++t) {
-      StatPartial p = partial[(size_t)iy * ntiles + t];
-      mn = fminf(mn, p.mn);
-      mx = fmaxf(mx, p.mx);
-      sum += p.sum;
-    }
-    slice_stats[3 * iy + 0] = mn;
-    slice_stats[3 * iy + 1] = mx;
-    slice_stats[3 * iy + 2] = (float)(sum / (double)count);
+// One block per slice: its tiles' partials are combined by a fixed tree (the
+// same thread always takes the same tiles), so the statistics are
+// deterministic; then one thread folds the slices in Y order exactly as
+// main.rs:1080-1092 does.
+__global__ void __launch_bounds__(256) slice_stats_kernel(const StatPartial *partial, int ntiles, int count,
+                                                          float *slice_stats) {
+  const int iy = blockIdx.x;
+  float mn = 3.40282347e+38f, mx = -3.40282347e+38f;
+  double sum = 0.0;
+  for (int t = threadIdx.x; t < ntiles; t += blockDim.x) {
+    const StatPartial p = partial[(size_t)iy * ntiles + t];
+    mn = fminf(mn, p.mn);
+    mx = fmaxf(mx, p.mx);
+    sum += p.sum;
   }
+  __shared__ float rmn[8], rmx[8];
+  __shared__ double rs[8];
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) { rmn[w] = mn; rmx[w] = mx; rs[w] = sum; }
   __syncthreads();
   if (threadIdx.x == 0) {
-    float gmin = 3.40282347e+38f, gmax = -3.40282347e+38f;
-    double gsum = 0.0;
-    for (int iy = 0; iy < ny; ++iy) {
-      float smin = slice_stats[3 * iy], smax = slice_stats[3 * iy + 1], smean = slice_stats[3 * iy + 2];
-      if (smin < gmin) gmin = smin;
-      if (smax > gmax) gmax = smax;
-      gsum += (double)smean * (double)count;
-    }
-    out3[0] = gmin;
-    out3[1] = gmax;
-    out3[2] = (float)(gsum / ((double)count * (double)ny));
+    for (int k = 1; k < 8; ++k) { mn = fminf(mn, rmn[k]); mx = fmaxf(mx, rmx[k]); }
+    double t = rs[0];
+    for (int k = 1; k < 8; ++k) t += rs[k];
+    mn = fminf(rmn[0], mn);
+    mx = fmaxf(rmx[0], mx);
+    slice_stats[3 * iy + 0] = mn;
+    slice_stats[3 * iy + 1] = mx;
+    slice_stats[3 * iy + 2] = (float)(t / (double)count);
   }
+}
+
+__global__ void fold_slices_kernel(const float *slice_stats, int ny, int count, float *out3) {
+  float gmin = 3.40282347e+38f, gmax = -3.40282347e+38f;
+  double gsum = 0.0;
+  for (int iy = 0; iy < ny; ++iy) {
+    const float smin = slice_stats[3 * iy], smax = slice_stats[3 * iy + 1], smean = slice_stats[3 * iy + 2];
+    if (smin < gmin) gmin = smin;
+    if (smax > gmax) gmax = smax;
+    gsum += (double)smean * (double)count;
+  }
+  out3[0] = gmin;
+  out3[1] = gmax;
+  out3[2] = (float)(gsum / ((double)count * (double)ny));
 }
 
 void launch_stats_reduce(const StatPartial *partial, int ny, int ntiles, int count,
                          float *slice_stats, float *out3, cudaStream_t st) {
-  stats_reduce_kernel<<<1, 1024, 0, st>>>(partial, ny, ntiles, count, slice_stats, out3);
+  slice_stats_kernel<<<ny, 256, 0, st>>>(partial, ntiles, count, slice_stats);
+  fold_slices_kernel<<<1, 1, 0, st>>>(slice_stats, ny, count, out3);
 }
 
 }  // namespace tg
