@@ -330,6 +330,7 @@ FpArgs fp_args(tg_session *s) {
   f.ocx = s->ocx;
   f.has_local = s->has_local;
   f.loc = local_dev(s);
+  f.fast = s->fp_fast ? 1 : 0;
   return f;
 }
 
@@ -470,6 +471,11 @@ int tg_session_create(const tg_geometry *g, const tg_options *opt, tg_session **
     zsmax = std::max(zsmax, fabsf(hv[i].sin_t * hv[i].zf));
   }
   s->fast = !s->has_local && !xt_any && zsmax <= 2.0f && fabsf(zsmax) == zsmax;
+  {
+    bool steep = false;  // the fast reprojector needs cos(tilt) > 0.05 in every view
+    for (int i = 0; i < s->nviews; ++i) steep |= !(hv[i].cos_t > 0.05f);
+    s->fp_fast = !s->has_local && !xt_any && !steep;
+  }
   if (s->zf_any && zsmax > 2.0f) s->fast = false;
   s->fmt = s->fast ? FMT_ROWPAIR : FMT_SINGLE;
 

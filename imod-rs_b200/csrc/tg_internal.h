@@ -117,6 +117,7 @@ struct FpArgs {
   float cx, cz, ocx;
   int has_local;
   LocalDev loc;
+  int fast;                 // no x-tilt, no local alignment, all cos > 0.05: fp_fast_kernel
 };
 void launch_reproject(const FpArgs &a, cudaStream_t st);
 

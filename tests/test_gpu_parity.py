@@ -122,6 +122,17 @@ def test_sirt_no_xtilt():
     assert rel_l2(vol, ref) <= TOL_FP32
 
 
+def test_sirt_bit_exact_without_filter():
+    # no R-weighting, no stretch: back-projection, reprojection (per-bin order of the
+    # reference's serial splat), residual and update are all exact f32 operations
+    nz, ny, nx = 13, 11, 40
+    proj = random_stack(nz, ny, nx, seed=30)
+    ang = angles(-60, 60, 10)
+    vol, _, ref, _ = both(proj, ang, sirt=2, sirt_relax=0.8, no_weight=True, no_cosine_stretch=True,
+                          thickness=22, width=44)
+    np.testing.assert_array_equal(vol, ref)
+
+
 def test_sirt_xtilt_log_fake():
     nz, ny, nx = 11, 10, 40
     proj = (smooth_stack(nz, ny, nx, seed=32) * 1000.0).astype(np.float32)
