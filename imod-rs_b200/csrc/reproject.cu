@@ -100,33 +100,57 @@ __global__ void __launch_bounds__(128) fp_kernel(FpArgs a) {
   *out = acc;
 }
 
-// Fast reprojection (no x-tilt, no local alignment, every view with cos > 0.05):
-// slice iy feeds only sinogram row iy, and a voxel's position x does not depend
-// on the slice, so one thread owns bin p of S consecutive rows and shares the
-// candidate search among them.  For each depth the columns whose exact
-// position lies in [p-1, p+1) are found by an estimate from 1/cos corrected
-// with exact evaluations (x is non-decreasing in the column), then visited in
-// increasing column order: the per-bin order (z ascending, x ascending) of the
-// reference's serial splat, so every bin is bit-identical to it.
-template <int S>
+// Fast reprojection (no local alignment, every view with cos(tilt)*cos(x-tilt)
+// > 0.05).  A voxel's position x does not depend on its slice, so one thread
+// owns bin p of S consecutive sinogram rows and shares the candidate search
+// among them.  For each depth the columns whose exact position lies in
+// [p-1, p+1) are found by an estimate from 1/cos corrected with exact
+// evaluations (x is non-decreasing in the column), then visited in increasing
+// column order.
+//
+// XT = false (no x-tilt): slice iy feeds only row iy, and the per-bin order
+// (z ascending, x ascending) is the reference's serial order, so every bin is
+// bit-identical to main.rs:831-896.
+//
+// XT = true: column ox moves the sample row by yoff = dx*sin(x-tilt), so slice
+// iy feeds rows floor(iy+yoff) and floor(iy+yoff)+1 with weights 1-f and f.
+// With n = floor(yoff), the thread's rows r0-1+i (i = 0..S) are the nominal
+// lower rows of slices iy_i = r0-1+i-n; f32 rounding of iy+yoff can only move
+// the floor one row up (then f = 0 and the slice feeds that row with weight 1).
+// The edge rules of the reference follow: a slice whose floor row is the last
+// row feeds it alone with weight 1 (the one-row branch), a floor row of -1
+// feeds nothing.  Weights and products are the reference's f32 expressions;
+// only the summation order differs (z, x, slice instead of slice, z, x).
+//
+// Grid: (views, bin blocks, row groups) -- the views of one row group run
+// together, so their reads of that slab of the volume hit L2.
+template <int S, bool XT, bool IL>
 __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r0 = blockIdx.y * S, v = blockIdx.z;
+  const int v = blockIdx.x;
+  const int p = blockIdx.y * blockDim.x + threadIdx.x;
+  const int r0 = blockIdx.z * S;
   if (p >= a.nx) return;
+  const int nrows = min(S, a.ny - r0);
+  if (v >= a.nviews) {  // views without a tilt angle contribute nothing (main.rs:683-686)
+    for (int s = 0; s < nrows; ++s) a.sino[((size_t)v * a.ny + r0 + s) * a.nx + p] = 0.0f;
+    return;
+  }
   const float4 g = __ldg(&a.vg[v]);
-  const float cos_t = g.x, sin_t = g.y, zf = g.z;
-  const float inv_a = 1.0f / cos_t;
+  const float cos_t = g.x, sin_t = g.y, zf = g.z, cos_xt = XT ? g.w : 1.0f;
+  const float sin_xt = XT ? __ldg(&a.vg2[v]).x : 0.0f;
+  const float inv_a = 1.0f / (cos_t * cos_xt);
   const float lo_t = (float)(p - 1), hi_t = (float)(p + 1);
   const size_t sstride = (size_t)a.onz * a.onx;
-  const float *vol0 = a.vol + (size_t)r0 * sstride;
-  int nrows = min(S, a.ny - r0);
   float acc[S];
 #pragma unroll
   for (int s = 0; s < S; ++s) acc[s] = 0.0f;
-  auto X = [&](int ox, float t2) {  // ((dx*cos)*1 + t2) + cx, exactly as main.rs:842
+  auto X = [&](int ox, float t2) {  // ((dx*cos)*cos_xt + t2) + cx, exactly as main.rs:842
     const float dx = __fsub_rn((float)ox, a.ocx);
-    return __fadd_rn(__fadd_rn(__fmul_rn(dx, cos_t), t2), a.cx);
+    const float t1 = XT ? __fmul_rn(__fmul_rn(dx, cos_t), cos_xt) : __fmul_rn(dx, cos_t);
+    return __fadd_rn(__fadd_rn(t1, t2), a.cx);
   };
+  // XT: row r0+s is the last row of the series (one-row branch) when s == last_s
+  const int last_s = a.ny - 1 - r0;
   for (int oz = 0; oz < a.onz; ++oz) {
     const float dz = __fsub_rn((float)oz, a.cz);
     const float t2 = __fmul_rn(__fmul_rn(dz, sin_t), zf);
@@ -135,7 +159,7 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
     lo = min(max(lo, 0), a.onx);
     while (lo > 0 && X(lo - 1, t2) >= lo_t) --lo;
     while (lo < a.onx && X(lo, t2) < lo_t) ++lo;
-    const float *vrow = vol0 + (size_t)oz * a.onx;
+    const float *vz = a.vol + (size_t)oz * a.onx;
     for (int ox = lo; ox < a.onx; ++ox) {
       const float x = X(ox, t2);
       if (!(x < hi_t)) break;
@@ -144,9 +168,49 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
       if ((unsigned)x0 > (unsigned)(a.nx - 2)) continue;  // px0 >= 0 && px0 + 1 < nx
       const float frac = __fsub_rn(x, __fsub_rn(tt, FMAGIC));
       const float w = x0 == p ? __fsub_rn(1.0f, frac) : frac;
+      if (!XT && IL) {
+        // interleaved copy: the S slices of this row group at (oz, ox) are contiguous
+        const float4 *q = reinterpret_cast<const float4 *>(a.volg) +
+                          (((size_t)blockIdx.z * a.onz + oz) * a.onx + ox) * (S / 4);
 #pragma unroll
-      for (int s = 0; s < S; ++s)
-        if (s < nrows) acc[s] = __fadd_rn(acc[s], __fmul_rn(__ldg(vrow + (size_t)s * sstride + ox), w));
+        for (int k = 0; k < S / 4; ++k) {
+          const float4 q4 = __ldg(q + k);
+          acc[4 * k + 0] = __fadd_rn(acc[4 * k + 0], __fmul_rn(q4.x, w));
+          acc[4 * k + 1] = __fadd_rn(acc[4 * k + 1], __fmul_rn(q4.y, w));
+          acc[4 * k + 2] = __fadd_rn(acc[4 * k + 2], __fmul_rn(q4.z, w));
+          acc[4 * k + 3] = __fadd_rn(acc[4 * k + 3], __fmul_rn(q4.w, w));
+        }
+      } else if (!XT) {
+        const float *vrow = vz + (size_t)r0 * sstride + ox;
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+          if (s < nrows) acc[s] = __fadd_rn(acc[s], __fmul_rn(__ldg(vrow + (size_t)s * sstride), w));
+      } else {
+        const float yoff = __fmul_rn(__fsub_rn((float)ox, a.ocx), sin_xt);
+        const float fn = floorf(yoff);
+        const int iy0 = r0 - 1 - (int)fn;  // slice of i = 0
+        const float *vcol = vz + ox;
+#pragma unroll
+        for (int i = 0; i <= S; ++i) {
+          const int iy = iy0 + i;
+          if (i > nrows || (unsigned)iy >= (unsigned)a.ny) continue;
+          const float A = (float)(r0 - 1 + i);  // nominal lower row
+          const float sy = __fadd_rn((float)iy, yoff);
+          const float fs = floorf(sy);
+          const bool nominal = fs == A;
+          const float syf = __fsub_rn(sy, fs);
+          const float c = __fmul_rn(__ldg(vcol + (size_t)iy * sstride), w);
+          // lower row A = r0-1+i -> acc[i-1]; upper row A+1 -> acc[i]
+          if (i >= 1 && nominal) {
+            const float wa = (i - 1 == last_s) ? 1.0f : __fsub_rn(1.0f, syf);
+            acc[i - 1] = __fadd_rn(acc[i - 1], __fmul_rn(c, wa));
+          }
+          if (i < nrows && !(r0 + i - 1 == -1 && nominal) && !(nominal && i - 1 == last_s)) {
+            const float wb = nominal ? syf : 1.0f;
+            acc[i] = __fadd_rn(acc[i], __fmul_rn(c, wb));
+          }
+        }
+      }
     }
   }
 #pragma unroll
@@ -154,11 +218,45 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
     if (s < nrows) a.sino[((size_t)v * a.ny + r0 + s) * a.nx + p] = acc[s];
 }
 
+// volg[g][oz][ox][j] = vol[g*G + j][oz][ox] (zero for rows past ny)
+template <int G>
+__global__ void interleave_kernel(const float *__restrict__ vol, float *__restrict__ volg, int ny,
+                                  int onz, int onx, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (g, oz, ox)
+  if (i >= n) return;
+  const size_t sl = (size_t)onz * onx;
+  const size_t g = i / sl, rem = i - g * sl;
+  float v[G];
+#pragma unroll
+  for (int j = 0; j < G; ++j) {
+    const size_t iy = g * G + j;
+    v[j] = iy < (size_t)ny ? __ldg(vol + iy * sl + rem) : 0.0f;
+  }
+  float4 *o = reinterpret_cast<float4 *>(volg) + i * (G / 4);
+#pragma unroll
+  for (int k = 0; k < G / 4; ++k) o[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+}
+
+template <int S>
+static void launch_fast(const FpArgs &a, cudaStream_t st) {
+  dim3 grid(a.nviews_all, (a.nx + 127) / 128, (a.ny + S - 1) / S);
+  if (a.fast == 2) {
+    fp_fast_kernel<S, true, false><<<grid, 128, 0, st>>>(a);
+  } else if (a.volg) {
+    const size_t n = (size_t)((a.ny + S - 1) / S) * a.onz * a.onx;
+    interleave_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.vol, a.volg, a.ny, a.onz, a.onx, n);
+    fp_fast_kernel<S, false, true><<<grid, 128, 0, st>>>(a);
+  } else {
+    fp_fast_kernel<S, false, false><<<grid, 128, 0, st>>>(a);
+  }
+}
+
+int fp_group_rows(int variant) { return variant == 1 || variant == 3 ? 16 : 8; }
+
 void launch_reproject(const FpArgs &a, cudaStream_t st) {
   if (a.fast) {
-    constexpr int S = 8;
-    dim3 grid((a.nx + 127) / 128, (a.ny + S - 1) / S, a.nviews);
-    fp_fast_kernel<S><<<grid, 128, 0, st>>>(a);
+    if (fp_group_rows(a.variant) == 16) launch_fast<16>(a, st);
+    else launch_fast<8>(a, st);
     return;
   }
   dim3 grid((a.nx + 127) / 128, a.ny, a.nviews_all);

@@ -125,7 +125,7 @@ static void free_session(tg_session *s) {
   if (!s) return;
   if (s->st) cudaStreamSynchronize(s->st);
   if (s->sirt_exec) cudaGraphExecDestroy(s->sirt_exec);
-  void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_mpart, s->d_pairs,
+  void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_mpart, s->d_pairs,
                   s->d_part, s->d_slice_stats, s->d_stats3, s->d_vg, s->d_vg2, s->d_weights,
                   s->d_conv, s->d_stretch, s->d_tw, s->d_err, s->d_lvinfo, s->d_lgoff, s->d_lxs,
                   s->d_lys, s->d_lgdx, s->d_lgdy};
@@ -330,7 +330,9 @@ FpArgs fp_args(tg_session *s) {
   f.ocx = s->ocx;
   f.has_local = s->has_local;
   f.loc = local_dev(s);
-  f.fast = s->fp_fast ? 1 : 0;
+  f.fast = s->fp_fast;
+  f.volg = s->d_volg;
+  f.variant = s->fp_variant;
   return f;
 }
 
@@ -472,9 +474,15 @@ int tg_session_create(const tg_geometry *g, const tg_options *opt, tg_session **
   }
   s->fast = !s->has_local && !xt_any && zsmax <= 2.0f && fabsf(zsmax) == zsmax;
   {
-    bool steep = false;  // the fast reprojector needs cos(tilt) > 0.05 in every view
-    for (int i = 0; i < s->nviews; ++i) steep |= !(hv[i].cos_t > 0.05f);
-    s->fp_fast = !s->has_local && !xt_any && !steep;
+    // the fast reprojector needs cos(tilt)*cos(x-tilt) > 0.05 in every view, and
+    // x-tilts whose row offsets are either zero or clearly above the reference's
+    // 1e-6 one-row threshold (|sin| >= 1e-5 with |dx| >= 0.5)
+    bool ok = !s->has_local;
+    for (int i = 0; i < s->nviews; ++i) {
+      ok &= hv[i].cos_t * hv[i].cos_xt > 0.05f;
+      ok &= hv[i].sin_xt == 0.0f || fabsf(hv[i].sin_xt) >= 1e-5f;
+    }
+    s->fp_fast = !ok ? 0 : xt_any ? 2 : 1;
   }
   if (s->zf_any && zsmax > 2.0f) s->fast = false;
   s->fmt = s->fast ? FMT_ROWPAIR : FMT_SINGLE;
@@ -553,6 +561,12 @@ int tg_session_create(const tg_geometry *g, const tg_options *opt, tg_session **
     return fail(rc);
   if (!opt->gpu_compat && opt->sirt_iters > 0 && (rc = dalloc(s, &s->d_sino, nproj * 4))) return fail(rc);
   if (!opt->gpu_compat && opt->fake_sirt > 0 && (rc = dalloc(s, &s->d_tmp, nvol * 4))) return fail(rc);
+  if (const char *e = getenv("TG_FP_VARIANT")) s->fp_variant = atoi(e) & 3;
+  if (!opt->gpu_compat && opt->sirt_iters > 0 && s->fp_fast == 1 && (s->fp_variant & 2)) {
+    const int G = fp_group_rows(s->fp_variant);
+    const size_t ng = (size_t)((s->ny + G - 1) / G) * G * s->onz * s->onx;
+    if ((rc = dalloc(s, &s->d_volg, ng * 4))) return fail(rc);
+  }
   if (s->has_local && (rc = upload_local(s, g->local, g->local ? g->n_local : 0, vg2))) return fail(rc);
   // zero the staging buffer once: rows past ny stay zero
   if ((ce = cudaMemsetAsync(s->d_pairs, 0, s->pairs_bytes, s->st)) != cudaSuccess) return fail(cuda_fail(ce, "memset"));

@@ -12,7 +12,10 @@ using tg::FMT_ROWPAIR;
 struct tg_session {  // one tilt series resident on a device
   int nx = 0, ny = 0, nz = 0, onx = 0, onz = 0, nviews = 0;
   tg_options o{};
-  bool has_local = false, fast = true, zf_any = false, fp_fast = false;
+  bool has_local = false, fast = true, zf_any = false;
+  int fp_fast = 0;  // reprojector: 0 general, 1 fast (no x-tilt), 2 fast with x-tilt
+  int fp_variant = 2;  // bit 0: 16 rows per thread, bit 1: interleaved volume copy
+  float *d_volg = nullptr;  // interleaved copy of the volume for the reprojector
   int fmt = FMT_ROWPAIR, store = TG_STORE_FP32;
   int padL = 0, PW = 0, rows_alloc = 0, variant = -1, ntiles_cap = 0;
   int dev = 0;

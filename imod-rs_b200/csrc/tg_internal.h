@@ -117,9 +117,12 @@ struct FpArgs {
   float cx, cz, ocx;
   int has_local;
   LocalDev loc;
-  int fast;                 // no x-tilt, no local alignment, all cos > 0.05: fp_fast_kernel
+  int fast;                 // fp_fast_kernel: 1 no x-tilt (bit-exact), 2 with x-tilt; 0 general
+  float *volg;              // fast == 1: row-group interleaved copy of vol, or null
+  int variant;              // bit 0: 16 rows per thread (else 8); bit 1: interleaved copy
 };
 void launch_reproject(const FpArgs &a, cudaStream_t st);
+int fp_group_rows(int variant);
 
 // ---- volume operations ----
 void launch_lowpass(float *vol, float *tmp, int onx, int onz, int ny, cudaStream_t st);

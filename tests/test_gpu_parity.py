@@ -133,6 +133,20 @@ def test_sirt_bit_exact_without_filter():
     np.testing.assert_array_equal(vol, ref)
 
 
+@pytest.mark.parametrize("ny", [10, 17])
+def test_sirt_xtilt_rows_and_edges(ny):
+    # x-tilt reprojection: rows shift by dx*sin(x-tilt) and split in two; edge rows
+    # take the reference's one-row branch; views with zero x-tilt stay one-row
+    nz, nx = 12, 48
+    proj = random_stack(nz, ny, nx, seed=40 + ny)
+    ang = angles(-55, 55, 10)
+    xt = np.linspace(-4.0, 4.0, nz).astype(np.float32)
+    xt[3] = 0.0
+    vol, _, ref, _ = both(proj, ang, sirt=2, sirt_relax=0.9, no_weight=True, no_cosine_stretch=True,
+                          xtilt=xt, thickness=20, width=52)
+    assert rel_l2(vol, ref) <= 1e-6
+
+
 def test_sirt_xtilt_log_fake():
     nz, ny, nx = 11, 10, 40
     proj = (smooth_stack(nz, ny, nx, seed=32) * 1000.0).astype(np.float32)
