@@ -15,27 +15,13 @@
 
 using namespace tg;
 
-struct tg_batch {
-  int dev = 0;
-  cudaStream_t st = nullptr;
-  std::vector<tg_session *> sess;
-  BpArgs *d_jobs = nullptr;
-  size_t jobs_cap = 0;
-  int4 *d_tiles = nullptr;
-  size_t tiles_cap = 0;
-  int *d_counter = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  tg_run_info info{};
-  int rounds = 0, persistent_launches = 0;
-};
-
 namespace tg {
 
 // One persistent launch per (storage, z-factor) group of fast-path series;
 // other series get their own launch.  ntiles[i] receives the partial-stat
 // tile count written for ss[i] (used when modes[i] == 0).
-static int batch_bp(tg_batch *b, const std::vector<tg_session *> &ss, const std::vector<int> &modes,
-                    std::vector<int> &ntiles, int *launches) {
+int batch_bp(tg_batch *b, const std::vector<tg_session *> &ss, const std::vector<int> &modes,
+             std::vector<int> &ntiles, int *launches) {
   ntiles.assign(ss.size(), 0);
   std::map<std::pair<int, int>, std::vector<int>> groups;
   for (size_t i = 0; i < ss.size(); ++i) {

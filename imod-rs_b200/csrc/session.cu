@@ -110,8 +110,21 @@ using namespace tg;
 
 namespace tg {
 
+// Sessions of the server allocate stream-ordered from its pool (a free does not
+// synchronise the device); a dry session only counts the bytes it would take.
 template <class T> static int dalloc(tg_session *s, T **p, size_t bytes) {
-  cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(bytes, 16));
+  if (s->dry) {
+    *p = nullptr;
+    s->dev_bytes += bytes;
+    return TG_OK;
+  }
+  if (s->fail_alloc) {
+    *p = nullptr;
+    set_error("device allocation failed (injected)");
+    return TG_ERR_OOM;
+  }
+  cudaError_t e = s->pool ? cudaMallocFromPoolAsync((void **)p, std::max<size_t>(bytes, 16), s->pool, s->own_st)
+                          : cudaMalloc((void **)p, std::max<size_t>(bytes, 16));
   if (e != cudaSuccess) {
     char buf[128];
     snprintf(buf, sizeof buf, "cudaMalloc(%zu bytes)", bytes);
@@ -123,6 +136,10 @@ template <class T> static int dalloc(tg_session *s, T **p, size_t bytes) {
 
 static void free_session(tg_session *s) {
   if (!s) return;
+  if (s->pool) {  // stream-ordered on the session's own stream
+    free_session_async(s, s->own_st);
+    return;
+  }
   if (s->st) cudaStreamSynchronize(s->st);
   if (s->sirt_exec) cudaGraphExecDestroy(s->sirt_exec);
   void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_mpart, s->d_pairs,
@@ -131,6 +148,20 @@ static void free_session(tg_session *s) {
                   s->d_lys, s->d_lgdx, s->d_lgdy};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  for (auto &e : s->ev)
+    if (e) cudaEventDestroy(e);
+  if (s->own_st) cudaStreamDestroy(s->own_st);
+  delete s;
+}
+
+void free_session_async(tg_session *s, cudaStream_t after) {
+  if (s->sirt_exec) cudaGraphExecDestroy(s->sirt_exec);  // freed on completion if in flight
+  void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_mpart, s->d_pairs,
+                  s->d_part, s->d_slice_stats, s->d_stats3, s->d_vg, s->d_vg2, s->d_weights,
+                  s->d_conv, s->d_stretch, s->d_tw, s->d_err, s->d_lvinfo, s->d_lgoff, s->d_lxs,
+                  s->d_lys, s->d_lgdx, s->d_lgdy};
+  for (void *p : ptrs)
+    if (p) cudaFreeAsync(p, after);
   for (auto &e : s->ev)
     if (e) cudaEventDestroy(e);
   if (s->own_st) cudaStreamDestroy(s->own_st);
@@ -191,6 +222,8 @@ static int upload_local(tg_session *s, const float *rows, int nrows, std::vector
   if ((rc = dalloc(s, &s->d_lys, ys_all.size() * sizeof(float)))) return rc;
   if ((rc = dalloc(s, &s->d_lgdx, gdx.size() * sizeof(float)))) return rc;
   if ((rc = dalloc(s, &s->d_lgdy, gdy.size() * sizeof(float)))) return rc;
+  if (s->dry) return TG_OK;
+  if (s->pool) TG_CUDA(cudaStreamSynchronize(s->own_st));  // the stream-ordered allocations exist
   TG_CUDA(cudaMemcpy(s->d_lvinfo, vinfo.data(), vinfo.size() * sizeof(int4), cudaMemcpyHostToDevice));
   TG_CUDA(cudaMemcpy(s->d_lgoff, goff.data(), goff.size() * sizeof(int), cudaMemcpyHostToDevice));
   if (!xs_all.empty()) TG_CUDA(cudaMemcpy(s->d_lxs, xs_all.data(), xs_all.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -313,6 +346,18 @@ int autotune(tg_session *s) {
   return TG_OK;
 }
 
+int tune_lookup(tg_session *s) {
+  if (!s->fast) return 0;
+  if (const char *env = getenv("TG_BP_VARIANT")) {
+    int v = atoi(env);
+    if (v >= 0 && v < bp_fast_variants()) return v;
+  }
+  auto key = std::make_tuple(s->nx, s->onx, s->onz, s->nviews, s->store, (int)s->zf_any, s->ny >= 64 ? 64 : s->ny);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(key);
+  return it != g_tune.end() ? it->second : -1;
+}
+
 FpArgs fp_args(tg_session *s) {
   FpArgs f{};
   f.vol = s->d_vol;
@@ -384,6 +429,7 @@ const char *tg_status_string(int st) {
     case TG_ERR_PANIC: return "input on which the reference panics";
     case TG_ERR_NOT_READY: return "not ready";
     case TG_ERR_NOT_FOUND: return "not found";
+    case TG_ERR_CANCELLED: return "cancelled";
     default: return "unknown status";
   }
 }
@@ -403,6 +449,16 @@ void tg_options_default(tg_options *o) {
 }
 
 int tg_session_create(const tg_geometry *g, const tg_options *opt, tg_session **out) {
+  return tg::session_create_ex(g, opt, nullptr, false, false, out);
+}
+
+}  // extern "C"
+
+// pool: allocate stream-ordered from it; dry: compute sizes only (no device
+// work; the returned object holds dev_bytes and must be freed with
+// session_discard); fail_alloc: fault-injection hook (the first allocation fails).
+int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPool_t pool, bool dry,
+                          bool fail_alloc, tg_session **out) {
   if (!g || !opt || !out) { set_error("null argument"); return TG_ERR_INVALID_ARG; }
   *out = nullptr;
   if (g->nx < 2 || g->ny < 1 || g->nz < 1 || g->nx > 65536 || g->ny > 65535 || g->nz > 4096) {
@@ -438,6 +494,9 @@ int tg_session_create(const tg_geometry *g, const tg_options *opt, tg_session **
   TG_CUDA(cudaSetDevice(opt->device));
 
   tg_session *s = new tg_session();
+  s->pool = pool;
+  s->dry = dry;
+  s->fail_alloc = fail_alloc;
   s->o = *opt;
   s->dev = opt->device;
   s->nx = g->nx;
@@ -531,11 +590,14 @@ int tg_session_create(const tg_geometry *g, const tg_options *opt, tg_session **
   s->use_conv = !fft_plan(s->nx, &s->plan);
   if (s->nx * 16 > 200 * 1024) { set_error("rows wider than 12800 are not supported"); return fail(TG_ERR_UNSUPPORTED); }
 
-  cudaError_t ce = cudaStreamCreateWithFlags(&s->own_st, cudaStreamNonBlocking);
-  if (ce != cudaSuccess) return fail(cuda_fail(ce, "cudaStreamCreate"));
-  s->st = s->own_st;
-  for (auto &e : s->ev)
-    if ((ce = cudaEventCreate(&e)) != cudaSuccess) return fail(cuda_fail(ce, "cudaEventCreate"));
+  cudaError_t ce = cudaSuccess;
+  if (!dry) {
+    ce = cudaStreamCreateWithFlags(&s->own_st, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) return fail(cuda_fail(ce, "cudaStreamCreate"));
+    s->st = s->own_st;
+    for (auto &e : s->ev)
+      if ((ce = cudaEventCreate(&e)) != cudaSuccess) return fail(cuda_fail(ce, "cudaEventCreate"));
+  }
 
   const size_t nproj = (size_t)s->nx * s->ny * s->nz;
   const size_t nvol = (size_t)s->onx * s->onz * s->ny;
@@ -568,6 +630,12 @@ int tg_session_create(const tg_geometry *g, const tg_options *opt, tg_session **
     if ((rc = dalloc(s, &s->d_volg, ng * 4))) return fail(rc);
   }
   if (s->has_local && (rc = upload_local(s, g->local, g->local ? g->n_local : 0, vg2))) return fail(rc);
+  if (dry) {
+    if (s->use_conv) s->dev_bytes += (size_t)s->nx * 4;
+    *out = s;
+    return TG_OK;
+  }
+  if (pool && (ce = cudaStreamSynchronize(s->st)) != cudaSuccess) return fail(cuda_fail(ce, "sync"));
   // zero the staging buffer once: rows past ny stay zero
   if ((ce = cudaMemsetAsync(s->d_pairs, 0, s->pairs_bytes, s->st)) != cudaSuccess) return fail(cuda_fail(ce, "memset"));
   if ((ce = cudaMemsetAsync(s->d_err, 0, 16, s->st)) != cudaSuccess) return fail(cuda_fail(ce, "memset"));
@@ -597,13 +665,18 @@ int tg_session_create(const tg_geometry *g, const tg_options *opt, tg_session **
       (ce = cudaMemcpy(s->d_stretch, stretch.data(), stretch.size() * 4, cudaMemcpyHostToDevice)))
     return fail(cuda_fail(ce, "cudaMemcpy(setup)"));
   if (!any_stretch) {
-    cudaFree(s->d_stretch);
+    if (pool) cudaFreeAsync(s->d_stretch, s->st);
+    else cudaFree(s->d_stretch);
     s->d_stretch = nullptr;
   }
   if ((ce = cudaStreamSynchronize(s->st)) != cudaSuccess) return fail(cuda_fail(ce, "sync"));
   *out = s;
   return TG_OK;
 }
+
+void tg::session_discard(tg_session *s) { free_session(s); }
+
+extern "C" {
 
 int tg_upload_projections(tg_session *s, const float *host, size_t n) {
   if (!s || !host) return TG_ERR_INVALID_ARG;

@@ -42,16 +42,25 @@ struct tg_session {  // one tilt series resident on a device
   cudaEvent_t ev[6] = {};
   cudaGraphExec_t sirt_exec = nullptr;
   float cx = 0, cz = 0, ocx = 0, inv_n = 0;
+  cudaMemPool_t pool = nullptr;  // stream-ordered allocations (server sessions)
+  bool dry = false, fail_alloc = false;
 };
 
 namespace tg {
 
+int session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPool_t pool, bool dry,
+                      bool fail_alloc, tg_session **out);
+void session_discard(tg_session *s);
+// frees the session's device memory stream-ordered after the work queued on `after`
+void free_session_async(tg_session *s, cudaStream_t after);
 LocalDev local_dev(tg_session *s);
 BpArgs bp_args(tg_session *s, int mode);
 FilterArgs filter_args(tg_session *s, bool residual);
 FpArgs fp_args(tg_session *s);
 int launch_bp(tg_session *s, int mode, int *ntiles);
 int autotune(tg_session *s);
+// the tile variant already tuned for this shape (or pinned by TG_BP_VARIANT), else -1
+int tune_lookup(tg_session *s);
 // log10 + means on first use, then the filter stage of the WBP pass
 int stage_front(tg_session *s, int *launches);
 // fake-SIRT passes, output transform (when the volume was stored raw) and statistics;
@@ -61,4 +70,26 @@ inline int sirt_iters(const tg_session *s) { return s->o.gpu_compat ? 0 : s->o.s
 inline int fake_passes(const tg_session *s) { return s->o.gpu_compat ? 0 : s->o.fake_sirt; }
 inline int first_mode(const tg_session *s) { return (sirt_iters(s) > 0 || fake_passes(s) > 0) ? 1 : 0; }
 
+// One persistent back-projection launch per (storage, z-factor) group of
+// fast-path series, on b->st; other series get their own launch.  ntiles[i]
+// receives the partial-stat tile count written for ss[i] (used when
+// modes[i] == 0).  Job and tile tables are copied stream-ordered, so calls may
+// follow each other on the same stream without waiting.
+int batch_bp(tg_batch *b, const std::vector<tg_session *> &ss, const std::vector<int> &modes,
+             std::vector<int> &ntiles, int *launches);
+
 }  // namespace tg
+
+struct tg_batch {
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  std::vector<tg_session *> sess;
+  tg::BpArgs *d_jobs = nullptr;
+  size_t jobs_cap = 0;
+  int4 *d_tiles = nullptr;
+  size_t tiles_cap = 0;
+  int *d_counter = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  tg_run_info info{};
+  int rounds = 0, persistent_launches = 0;
+};

@@ -21,7 +21,7 @@ TG_OK = 0
 STATUS = {0: "ok", -1: "invalid argument", -2: "out of device memory", -3: "CUDA error",
           -4: "device wait timed out", -5: "over memory budget", -6: "unsupported",
           -7: "no sm_100 CUDA device", -8: "input on which the reference panics",
-          -9: "not ready", -10: "not found"}
+          -9: "not ready", -10: "not found", -11: "cancelled"}
 FILL = {"mean": 0, "zero": 1, "edge": 2}
 STORAGE = {"fp32": 0, "fp16": 1, "bf16": 2}
 
@@ -67,6 +67,28 @@ class MrcInfo(C.Structure):
                 ("swapped", _i32), ("xlen", _f), ("ylen", _f), ("zlen", _f), ("amin", _f),
                 ("amax", _f), ("amean", _f), ("nlabl", _i32), ("imod", _i32),
                 ("header", C.c_uint8 * 1024)]
+
+
+class Job(C.Structure):
+    _fields_ = [("geometry", Geometry), ("options", Options), ("projections", _P),
+                ("n_projections", C.c_size_t), ("volume_out", _P), ("tag", C.c_uint64)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("state", _i32), ("status", _i32), ("stats", Stats), ("rounds", _i32),
+                ("submit_ms", C.c_double), ("admit_ms", C.c_double), ("done_ms", C.c_double),
+                ("updates", C.c_double), ("device_bytes", C.c_uint64), ("tag", C.c_uint64)]
+
+
+class ServerInfo(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("queued", C.c_uint64), ("running", C.c_uint64), ("budget_bytes", C.c_uint64),
+                ("bytes_in_use", C.c_uint64), ("bytes_peak", C.c_uint64), ("rounds", C.c_uint64),
+                ("bp_launches", C.c_uint64), ("updates_done", C.c_double)]
+
+
+JOB_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
+FAULT_ALLOC, FAULT_ADMIT = 1, 2
 
 
 class TiltGpuError(RuntimeError):
@@ -116,6 +138,14 @@ EXPORTS = {
     "tg_tilt_output_header": (C.c_int, [_P, _i32, _i32, _P]),
     "tg_read_tilt_file": (C.c_int, [C.c_char_p, _P, _i32, C.POINTER(_i32)]),
     "tg_write_tilt_file": (C.c_int, [C.c_char_p, _P, _i32]),
+    "tg_server_create": (C.c_int, [_i32, C.c_uint64, _i32, C.POINTER(_P)]),
+    "tg_server_submit": (C.c_int, [_P, C.POINTER(Job), C.POINTER(C.c_uint64)]),
+    "tg_server_poll": (C.c_int, [_P, C.c_uint64, C.POINTER(JobResult)]),
+    "tg_server_wait": (C.c_int, [_P, C.c_uint64, _i32, C.POINTER(JobResult)]),
+    "tg_server_release": (C.c_int, [_P, C.c_uint64]),
+    "tg_server_get_info": (C.c_int, [_P, C.POINTER(ServerInfo)]),
+    "tg_server_inject": (C.c_int, [_P, _i32, _i32]),
+    "tg_server_destroy": (C.c_int, [_P]),
 }
 # library-internal helpers exported for tests and the benchmark (not in the header)
 EXTRA = {
@@ -329,6 +359,108 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def _geometry(nx, ny, nz, angles, width, thickness, xtilt, zfactor, local, keep):
+    ang, xt, zf = _f32(angles), _f32(xtilt), _f32(zfactor)
+    loc = None if local is None else _f32(np.asarray(local).reshape(-1, 5))
+    keep += [ang, xt, zf, loc]
+    g = Geometry()
+    g.nx, g.ny, g.nz = int(nx), int(ny), int(nz)
+    g.out_nx = int(width or 0)
+    g.out_nz = int(thickness or 0)
+    g.n_angles, g.angles = len(ang), _fptr(ang)
+    if xt is not None:
+        g.n_xtilt, g.xtilt = len(xt), _fptr(xt)
+    if zf is not None:
+        g.n_zfactor, g.zfactor = len(zf), _fptr(zf)
+    if loc is not None:
+        g.n_local, g.local, g.has_local = len(loc), _fptr(loc), 1
+    return g
+
+
+def _result(r: JobResult):
+    return {"state": JOB_STATES.get(r.state, r.state), "status": r.status,
+            "stats": {"amin": r.stats.amin, "amax": r.stats.amax, "amean": r.stats.amean},
+            "rounds": r.rounds, "submit_ms": r.submit_ms, "admit_ms": r.admit_ms,
+            "done_ms": r.done_ms, "updates": r.updates, "device_bytes": r.device_bytes,
+            "tag": r.tag}
+
+
+class Server:
+    """Request loop with continuous batching (tg_server_*).  Jobs are submitted
+    from any thread; their projection arrays (and output arrays) are kept alive
+    here until the job is released."""
+
+    def __init__(self, device=0, budget_bytes=0, max_active=64):
+        self.h = _P()
+        check(lib().tg_server_create(device, int(budget_bytes), int(max_active), C.byref(self.h)))
+        self._keep = {}
+
+    def submit(self, proj, angles, *, out=None, width=None, thickness=0, xtilt=None, zfactor=None,
+               local=None, tag=0, **opts):
+        """proj: float32 (nz, ny, nx) host array (pinned memory copies fastest);
+        out: float32 host array of the output volume (ny, thickness, width) or None."""
+        nz, ny, nx = proj.shape
+        keep = [proj, out]
+        p = proj if (proj.dtype == np.float32 and proj.flags.c_contiguous) else _f32(proj)
+        keep.append(p)
+        if out is not None and not (out.dtype == np.float32 and out.flags.c_contiguous and out.flags.writeable):
+            raise ValueError("out must be a writeable C-contiguous float32 array")
+        j = Job()
+        j.geometry = _geometry(nx, ny, nz, angles, width, thickness, xtilt, zfactor, local, keep)
+        j.options = make_options(**opts)
+        j.projections = p.ctypes.data
+        j.n_projections = p.size
+        j.volume_out = None if out is None else out.ctypes.data
+        j.tag = int(tag)
+        jid = C.c_uint64()
+        check(lib().tg_server_submit(self.h, C.byref(j), C.byref(jid)))
+        self._keep[jid.value] = keep
+        return jid.value
+
+    def poll(self, jid):
+        r = JobResult()
+        check(lib().tg_server_poll(self.h, jid, C.byref(r)))
+        return _result(r)
+
+    def wait(self, jid, timeout_ms=-1):
+        r = JobResult()
+        rc = lib().tg_server_wait(self.h, jid, int(timeout_ms), C.byref(r))
+        if rc == -9:
+            return None
+        check(rc)
+        return _result(r)
+
+    def release(self, jid):
+        check(lib().tg_server_release(self.h, jid))
+        self._keep.pop(jid, None)
+
+    def info(self):
+        i = ServerInfo()
+        check(lib().tg_server_get_info(self.h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in ServerInfo._fields_}
+
+    def inject(self, fault, count=1):
+        check(lib().tg_server_inject(self.h, int(fault), int(count)))
+
+    def close(self):
+        if self.h:
+            lib().tg_server_destroy(self.h)
+            self.h = _P()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def reconstruct(proj, angles, **kw):

@@ -36,8 +36,9 @@ typedef enum {
   TG_ERR_NO_DEVICE = -7,    /* no CUDA device / not sm_100 */
   TG_ERR_PANIC = -8,        /* input on which the reference panics (e.g. fewer
                                tilt angles than views with cosine stretch on) */
-  TG_ERR_NOT_READY = -9,    /* tg_poll: job still running */
-  TG_ERR_NOT_FOUND = -10    /* unknown job id */
+  TG_ERR_NOT_READY = -9,    /* tg_server_wait: job still running */
+  TG_ERR_NOT_FOUND = -10,   /* unknown job id */
+  TG_ERR_CANCELLED = -11    /* job dropped by tg_server_destroy before admission */
 } tg_status;
 
 /* Fill modes of apps/tilt/src/main.rs:122-128 */
@@ -157,6 +158,66 @@ int tg_batch_reconstruct(tg_batch *b);
 int tg_batch_synchronize(tg_batch *b);
 int tg_batch_last_run(tg_batch *b, tg_run_info *info);
 int tg_batch_destroy(tg_batch *b);
+
+/* ---- Serving: a request loop with continuous batching (no counterpart in the
+ * reference, which reconstructs one series per process) ----
+ * Jobs (WBP or SIRT, any size) are submitted from any thread.  One device
+ * thread per server admits them first-in first-out while the device bytes of the
+ * admitted jobs stay within the budget and fewer than max_active run, copies
+ * their projections in on a copy stream, and runs rounds: every round takes each
+ * running job one step further (its filter + WBP pass, or one SIRT
+ * reproject/residual/update) with the back-projections of all those jobs in one
+ * persistent launch; jobs join and leave at round boundaries.  A finished job's
+ * volume is copied out on a third stream and its memory returns to the server's
+ * stream-ordered pool.  Each job's result is identical to tg_reconstruct of the
+ * same series alone.  A device error word set by a job's kernels fails that job
+ * only. */
+typedef struct tg_server tg_server;
+typedef enum { TG_JOB_QUEUED = 0, TG_JOB_RUNNING = 1, TG_JOB_DONE = 2, TG_JOB_FAILED = 3 } tg_job_state;
+typedef struct {
+  tg_geometry geometry;     /* copied at submit (the arrays may be freed afterwards) */
+  tg_options options;       /* options.device is ignored (the server's device) */
+  const float *projections; /* host, nx*ny*nz floats; must stay valid until the job ends */
+  size_t n_projections;
+  float *volume_out;        /* host, ny*out_nz*out_nx floats (slice-major), or NULL; written
+                               before the job reports TG_JOB_DONE.  Pinned memory copies fastest. */
+  uint64_t tag;             /* returned in tg_job_result */
+} tg_job;
+typedef struct {
+  int32_t state;            /* tg_job_state */
+  int32_t status;           /* TG_OK, or the failure of a TG_JOB_FAILED job */
+  tg_stats stats;           /* header statistics (main.rs:1080-1093) of a done job */
+  int32_t rounds;           /* 1 + SIRT iterations */
+  double submit_ms, admit_ms, done_ms;  /* server clock (ms since tg_server_create); -1 if not yet */
+  double updates;           /* voxel-view updates of the job */
+  uint64_t device_bytes;    /* device memory the job held while running */
+  uint64_t tag;
+} tg_job_result;
+typedef struct {
+  uint64_t submitted, completed, failed, queued, running;
+  uint64_t budget_bytes, bytes_in_use, bytes_peak;
+  uint64_t rounds, bp_launches;
+  double updates_done;
+} tg_server_info;
+typedef enum {
+  TG_FAULT_ALLOC = 1,  /* the next `count` admissions fail their device allocation (TG_ERR_OOM) */
+  TG_FAULT_ADMIT = 2   /* the next `count` admissions are refused (TG_ERR_BUDGET) */
+} tg_fault;
+/* budget_bytes 0: 80% of the device's free memory; max_active <= 0: 64. */
+int tg_server_create(int32_t device, uint64_t budget_bytes, int32_t max_active, tg_server **out);
+/* TG_ERR_BUDGET if the job alone exceeds the budget; other validation errors as tg_session_create. */
+int tg_server_submit(tg_server *sv, const tg_job *job, uint64_t *id);
+/* Current state of a job (TG_OK), or TG_ERR_NOT_FOUND. */
+int tg_server_poll(tg_server *sv, uint64_t id, tg_job_result *out);
+/* Waits up to timeout_ms (<0: no limit) for the job to end; TG_ERR_NOT_READY on timeout. */
+int tg_server_wait(tg_server *sv, uint64_t id, int32_t timeout_ms, tg_job_result *out);
+/* Forgets an ended job's record; TG_ERR_NOT_READY while it runs. */
+int tg_server_release(tg_server *sv, uint64_t id);
+int tg_server_get_info(tg_server *sv, tg_server_info *out);
+/* Host-side fault injection (tg_fault); no device fault is ever injected. */
+int tg_server_inject(tg_server *sv, int32_t fault, int32_t count);
+/* Drops queued jobs (TG_ERR_CANCELLED), lets running jobs finish, stops the device thread. */
+int tg_server_destroy(tg_server *sv);
 
 /* ---- The reference's GPU seam, same arguments and meaning ----
  * GpuSession::new(projections, tilt_cos_sin, in_nx, in_ny, n_projs, out_nx, out_nz)
