@@ -365,6 +365,213 @@ def run_reference(args):
         dist.destroy_process_group()
 
 
+def c4_jobs(n=64, seed=4):
+    """Batched uneven series: width in {256,384,512,768,1024} (square projections),
+    views U{41..121}, ranges +-U(50,70) deg with uneven steps, thickness U{100..500},
+    WBP:SIRT(10) = 3:1, each with its own seeded phantom and noise level."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(n):
+        w = int(rng.choice([256, 384, 512, 768, 1024]))
+        nv = int(rng.integers(41, 122))
+        rmax = float(rng.uniform(50, 70))
+        steps = rng.uniform(0.5, 1.5, nv - 1)
+        steps = steps / steps.sum() * 2 * rmax
+        ang = (-rmax + np.concatenate([[0.0], np.cumsum(steps)])).astype(np.float32)
+        thick = int(rng.integers(100, 501))
+        jobs.append(dict(w=w, nv=nv, ang=ang, thick=thick, sirt=10 if i % 4 == 3 else 0,
+                         seed=1000 + i, noise=float(rng.uniform(0.2, 0.8))))
+    return jobs
+
+
+def job_updates(j):
+    return float(j["w"]) * j["w"] * j["thick"] * len(j["ang"]) * (1 + 2 * j["sirt"])
+
+
+def synth_job(T, torch, j, device_only=False):
+    """Seeded ellipsoid phantom projections of one job (device tensor, or pinned host)."""
+    ne = max(10, int(300 * (j["w"] / 512) ** 2 * j["thick"] / 200))
+    d = torch.empty((len(j["ang"]), j["w"], j["w"]), dtype=torch.float32, device="cuda")
+    T.synth_projections(j["ang"], nx=j["w"], ny=j["w"], vol_nz=j["thick"], n_ell=ne,
+                        n_beads=max(4, ne // 8), noise_kind=1, noise=j.get("noise", 0.5),
+                        seed=j["seed"], out_device_ptr=d.data_ptr())
+    if device_only:
+        return d
+    h = torch.empty(d.shape, dtype=torch.float32, pin_memory=True)
+    h.copy_(d)
+    del d
+    return h
+
+
+def run_c4(args):
+    """64 uneven series: one persistent launch per round (FP16 staging, FP32
+    accumulation) against the plain FP32 form (one series at a time)."""
+    import torch
+
+    import tiltgpu as T
+    torch.cuda.set_device(0)
+    jobs = c4_jobs()
+    projs = [synth_job(T, torch, j, device_only=True) for j in jobs]
+    upd = sum(job_updates(j) for j in jobs)
+
+    def sessions(storage):
+        out = []
+        for j, d in zip(jobs, projs):
+            s = T.Session(j["w"], j["w"], len(j["ang"]), j["ang"], thickness=j["thick"], sirt=j["sirt"],
+                          radial=(0.35, 0.035), storage=storage)
+            s.set_device(d.data_ptr(), d.numel())
+            out.append(s)
+        return out
+
+    res = {}
+    ss = sessions("fp32")
+    for s in ss:  # tunes every shape once
+        s.reconstruct()
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s in ss:
+            s.reconstruct(sync=True)
+        times.append(time.perf_counter() - t0)
+    res["plain_fp32"] = upd / min(times)
+    for s in ss:
+        s.close()
+    for storage in ("fp16", "fp32"):
+        ss = sessions(storage)
+        b = T.Batch()
+        for s in ss:
+            b.add(s)
+        b.reconstruct()
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            b.reconstruct()
+            times.append(time.perf_counter() - t0)
+        res["batched_" + storage] = upd / min(times)
+        b.close()
+        for s in ss:
+            s.close()
+    line = {"metric": METRIC, "value": res["batched_fp16"], "unit": "updates/s", "n_gpus": 1,
+            "workload": "c4: 64 uneven series, WBP:SIRT(10) 3:1, one persistent launch per round",
+            "plain_fp32": res["plain_fp32"], "batched_fp32": res["batched_fp32"],
+            "batched_fp16_over_plain_fp32": res["batched_fp16"] / res["plain_fp32"],
+            "updates_per_step": upd, "steps": args.steps, "timing": "best of steps, wall clock with sync",
+            "data": "synthetic seeded phantoms, projections resident in HBM"}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """Poisson request stream through tg_server (continuous batching, HBM admission
+    budget) with p50/p99 latency; beside it the same arrivals served one at a time
+    by plain FP32 sessions (each pool series timed once end to end, the arrivals
+    replayed through one first-in first-out server with those service times)."""
+    import torch
+
+    import tiltgpu as T
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(20)
+    small = c4_jobs(args.pool, seed=5)
+    big_ang = np.arange(-60, 61, 1.0).astype(np.float32)
+    large = [dict(w=2048, nv=121, ang=big_ang, thick=800, sirt=0, seed=9000 + k, noise=0.5) for k in range(2)]
+    t0 = time.perf_counter()
+    pool = [(j, synth_job(T, torch, j)) for j in small + large]
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    print(f"# pool of {len(pool)} seeded series ready in {time.perf_counter() - t0:.1f}s", file=sys.stderr,
+          flush=True)
+    arrivals, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / args.rate)
+        if t >= args.duration:
+            break
+        if rng.random() < args.large_frac:
+            k = len(small) + int(rng.integers(0, len(large)))
+        else:
+            k = int(rng.integers(0, len(small)))
+        arrivals.append((t, k))
+    # pinned output rings: every result is copied out; contents are not checked here
+    max_small = max(j["w"] * j["w"] * j["thick"] for j in small)
+    ring_small = [torch.empty(max_small, dtype=torch.float32, pin_memory=True) for _ in range(4)]
+    ring_large = torch.empty(2048 * 2048 * 800, dtype=torch.float32, pin_memory=True)
+
+    def out_for(i, j):
+        n = j["w"] * j["w"] * j["thick"]
+        buf = ring_large if j["w"] == 2048 else ring_small[i % len(ring_small)]
+        return buf[:n].numpy().reshape(j["w"], j["thick"], j["w"])
+
+    def kw_of(j, storage, sirt=None):
+        return dict(thickness=j["thick"], sirt=j["sirt"] if sirt is None else sirt, radial=(0.35, 0.035),
+                    storage=storage)
+
+    # tune the tile shape of every pool shape (both forms) outside the timed stream
+    for j, h in pool:
+        for storage in ("fp16", "fp32"):
+            with T.Session(j["w"], j["w"], len(j["ang"]), j["ang"], **kw_of(j, storage, sirt=0)) as s:
+                s.upload(h.numpy())
+                s.reconstruct()
+    torch.cuda.empty_cache()
+    sampler = ClockSampler(0)
+    sv = T.Server(device=0, budget_bytes=int(args.budget_gb * 1e9), max_active=64)
+    ids = []
+    sampler.start()
+    start = time.perf_counter()
+    for i, (ta, k) in enumerate(arrivals):
+        now = time.perf_counter() - start
+        if ta > now:
+            time.sleep(ta - now)
+        j, h = pool[k]
+        ids.append(sv.submit(h.numpy(), j["ang"], out=out_for(i, j), tag=k, **kw_of(j, "fp16")))
+    results = [sv.wait(jid) for jid in ids]
+    wall = time.perf_counter() - start
+    clocks = sampler.stop()
+    info = sv.info()
+    sv.close()
+    done = [r for r in results if r["state"] == "done"]
+    lat = np.array([r["done_ms"] - r["submit_ms"] for r in done])
+    span_ms = max(r["done_ms"] for r in done) - min(r["submit_ms"] for r in done)
+    upd = sum(r["updates"] for r in done)
+    service = []
+    for i, (j, h) in enumerate(pool):
+        out = out_for(i, j)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        with T.Session(j["w"], j["w"], len(j["ang"]), j["ang"], **kw_of(j, "fp32")) as s:
+            s.upload(h.numpy())
+            s.reconstruct()
+            s.download(out=out)
+        service.append(time.perf_counter() - t1)
+    free_at, serial_lat = 0.0, []
+    for ta, k in arrivals:
+        begin = max(ta, free_at)
+        free_at = begin + service[k]
+        serial_lat.append(free_at - ta)
+    arr_upd = sum(job_updates(pool[k][0]) for _, k in arrivals)
+    serial_busy = sum(service[k] for _, k in arrivals)
+    line = {"metric": METRIC, "value": upd / (span_ms / 1e3), "unit": "updates/s", "n_gpus": 1,
+            "workload": (f"serve: Poisson {args.rate} jobs/s for {args.duration:.0f} s, C4 sizes "
+                         f"({len(small)} seeded series) + {args.large_frac:.0%} 2048^2x121-view WBP jobs "
+                         f"(thickness 800), FP16 staging, budget {args.budget_gb:.0f} GB"),
+            "jobs": len(arrivals), "done": len(done), "failed": len(results) - len(done),
+            "failures": sorted({f'{r["status"]}: {r["message"]}' for r in results if r["state"] != "done"})[:5],
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "max": float(lat.max())},
+            "wall_s": wall, "rounds": info["rounds"], "bp_launches": info["bp_launches"],
+            "gpu_round_s": info["gpu_round_ms"] / 1e3, "host_round_s": info["host_round_ms"] / 1e3,
+            "host_admit_s": info["host_admit_ms"] / 1e3, "oom_requeues": info["oom_requeues"],
+            "bytes_peak": info["bytes_peak"],
+            "device_busy_updates_per_s": upd / max(info["gpu_round_ms"] / 1e3, 1e-9),
+            "serial_plain_fp32": {"value": arr_upd / serial_busy, "unit": "updates/s",
+                                  "utilisation": serial_busy / args.duration,
+                                  "latency_ms_fifo_replay": {
+                                      "p50": float(np.percentile(serial_lat, 50)) * 1e3,
+                                      "p99": float(np.percentile(serial_lat, 99)) * 1e3},
+                                  "how": "each pool series timed once end to end (upload, reconstruct, "
+                                         "download); the arrivals replayed through one FIFO server"},
+            "clocks": clocks, "data": "synthetic seeded phantoms, projections from pinned host memory"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -372,7 +579,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "serve"])
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
+    ap.add_argument("--duration", type=float, default=120.0, help="serve: seconds of arrivals")
+    ap.add_argument("--large-frac", type=float, default=0.05, help="serve: share of 2048^2 jobs")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM admission budget")
+    ap.add_argument("--pool", type=int, default=32, help="serve: distinct seeded C4-size series")
     ap.add_argument("--forms", default="fp32,fp16", help="staging precisions to time")
     ap.add_argument("--profile", action="store_true",
                     help="time the requested forms only (no e2e, no CPU baseline); for ncu captures")
@@ -381,6 +593,12 @@ def main():
         ap.error("--forms other than fp32,fp16 needs --profile")
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "c4":
+        run_c4(args)
+        return
+    if args.workload == "serve":
+        run_serve(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -513,30 +513,39 @@ __global__ void __launch_bounds__(NT + 32) bp_fast_kernel(const __grid_constant_
 // arithmetic is the same as in the per-series kernel, so every series' result
 // does not depend on what else is in the batch.
 template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
-__global__ void __launch_bounds__(NT + 32) bp_batch_kernel(const BpArgs *__restrict__ jobs,
-                                                           const int4 *__restrict__ tiles, int ntiles,
-                                                           int *counter, int max_views) {
+__global__ void __launch_bounds__(NT + 32) bp_batch_kernel(const BpArgs *__restrict__ jobs, int njobs,
+                                                           int ntiles, int *counter, int max_views) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ volatile int s_abort;
-  __shared__ int s_tile;
+  __shared__ int4 s_tile;  // (tile, series, index inside the series, -)
   __shared__ __align__(16) BpArgs s_args;
   const SmemLayout<C> L(sm, max_views);
   init_ring(L, &s_abort);
   int gst = 0;
   for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
+    if (threadIdx.x == 0) {
+      const int t = atomicAdd(counter, 1);
+      int lo = 0, hi = njobs - 1;  // last series whose first tile is <= t
+      while (t < ntiles && lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&jobs[mid].tile0) <= t) lo = mid;
+        else hi = mid - 1;
+      }
+      s_tile = make_int4(t, lo, t < ntiles ? t - __ldg(&jobs[lo].tile0) : 0, 0);
+    }
     __syncthreads();
-    const int t = s_tile;
-    if (t >= ntiles || s_abort) break;
-    const int4 T = tiles[t];  // (job, bx, by, bz)
+    const int4 T = s_tile;
+    if (T.x >= ntiles || s_abort) break;
     {
-      const uint32_t *src = reinterpret_cast<const uint32_t *>(&jobs[T.x]);
+      const uint32_t *src = reinterpret_cast<const uint32_t *>(&jobs[T.y]);
       uint32_t *dst = reinterpret_cast<uint32_t *>(const_cast<BpArgs *>(&s_args));
       for (int i = threadIdx.x; i < (int)(sizeof(BpArgs) / 4); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
-    if (!bp_tile<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>(s_args, T.y, T.z, T.w, sm, L, gst, &s_abort)) {
+    const int nbx = s_args.nbx, nxz = s_args.ntiles_xz;
+    const int bx = T.z % nbx, by = (T.z % nxz) / nbx, bz = T.z / nxz;
+    if (!bp_tile<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>(s_args, bx, by, bz, sm, L, gst, &s_abort)) {
       s_abort = 1;
     }
   }
@@ -594,7 +603,7 @@ static int launch_batch_t(const BatchLaunch &bl, cudaStream_t st) {
   const int grid = std::max(1, std::min(bl.ntiles, nsm * std::max(1, per_sm)));
   e = cudaMemsetAsync(bl.counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(tile counter)");
-  kern<<<grid, C::NTHR, smem, st>>>(bl.jobs, bl.tiles, bl.ntiles, bl.counter, bl.max_views);
+  kern<<<grid, C::NTHR, smem, st>>>(bl.jobs, bl.njobs, bl.ntiles, bl.counter, bl.max_views);
   return TG_OK;
 }
 

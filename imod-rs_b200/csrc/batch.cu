@@ -40,38 +40,32 @@ int batch_bp(tg_batch *b, const std::vector<tg_session *> &ss, const std::vector
     int S, TX, TZ;
     bp_fast_tile_shape(variant, &S, &TX, &TZ);
     std::vector<BpArgs> jobs;
-    std::vector<int4> tiles;
+    long long total = 0;
     int max_views = 1;
     for (int i : idx) {
       BpArgs a = bp_args(ss[i], modes[i]);
       a.nbx = (a.onx + TX - 1) / TX;
       const int nbz = (a.onz + TZ - 1) / TZ, nby = (a.ny + S - 1) / S;
       a.ntiles_xz = a.nbx * nbz;
+      a.tile0 = (int)total;
+      total += (long long)a.ntiles_xz * nby;
       ntiles[i] = a.ntiles_xz;
-      const int j = (int)jobs.size();
       jobs.push_back(a);
       max_views = std::max(max_views, a.nviews);
-      for (int bz = 0; bz < nby; ++bz)
-        for (int by = 0; by < nbz; ++by)
-          for (int bx = 0; bx < a.nbx; ++bx) tiles.push_back(make_int4(j, bx, by, bz));
     }
+    if (total >= (1ll << 31) - (1ll << 20)) { set_error("too many tiles in one batch"); return TG_ERR_UNSUPPORTED; }
     if (jobs.size() > b->jobs_cap) {
-      cudaFree(b->d_jobs);
-      b->jobs_cap = std::max<size_t>(jobs.size(), 2 * b->jobs_cap);
+      cudaFree(b->d_jobs);  // synchronises: earlier launches may still read the table
+      b->jobs_cap = std::max<size_t>(std::max<size_t>(jobs.size(), 64), 2 * b->jobs_cap);
       TG_CUDA(cudaMalloc(&b->d_jobs, b->jobs_cap * sizeof(BpArgs)));
     }
-    if (tiles.size() > b->tiles_cap) {
-      cudaFree(b->d_tiles);
-      b->tiles_cap = std::max<size_t>(tiles.size(), 2 * b->tiles_cap);
-      TG_CUDA(cudaMalloc(&b->d_tiles, b->tiles_cap * sizeof(int4)));
-    }
-    // pageable sources: the copies have read the vectors when these calls return
+    // stream-ordered after the previous launch that read the table; the pageable
+    // source has been staged when the call returns
     TG_CUDA(cudaMemcpyAsync(b->d_jobs, jobs.data(), jobs.size() * sizeof(BpArgs), cudaMemcpyHostToDevice, b->st));
-    TG_CUDA(cudaMemcpyAsync(b->d_tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice, b->st));
     BatchLaunch bl{};
     bl.jobs = b->d_jobs;
-    bl.tiles = b->d_tiles;
-    bl.ntiles = (int)tiles.size();
+    bl.njobs = (int)jobs.size();
+    bl.ntiles = (int)total;
     bl.counter = b->d_counter;
     bl.max_views = max_views;
     int rc = launch_bp_batch(bl, kv.first.first, kv.first.second != 0, variant, b->st);
@@ -223,7 +217,6 @@ int tg_batch_destroy(tg_batch *b) {
   cudaSetDevice(b->dev);
   cudaStreamSynchronize(b->st);
   cudaFree(b->d_jobs);
-  cudaFree(b->d_tiles);
   cudaFree(b->d_counter);
   cudaEventDestroy(b->ev0);
   cudaEventDestroy(b->ev1);

@@ -1,28 +1,31 @@
 // server.cu -- request loop with continuous batching over one device.
 //
 // Threads: any number of client threads call tg_server_submit / poll / wait;
-// one device thread owns every CUDA call of the server.  Streams: `cs` runs
-// the rounds (filter, reprojection, batched back-projection, statistics),
-// `us` copies projections in, `ds` copies volumes and statistics out.
+// an admission thread creates the sessions of admitted jobs and starts their
+// copies in; the device thread issues the rounds and collects finished jobs.
+// Streams: `cs` runs the rounds (filter, reprojection, batched back-projection,
+// statistics), `us` copies projections in, `ds` copies volumes and statistics
+// out, `fs` returns memory to the pool.
 //
-// Device thread loop:
-//   1. finished jobs (their copy-out event has completed) report DONE/FAILED,
-//      and their memory goes back to the pool (stream-ordered free on `ds`);
-//   2. admission, first-in first-out: the head job is admitted while the
+//   1. (device thread) finished jobs -- their copy-out event has completed --
+//      report DONE/FAILED and their memory is freed stream-ordered on `fs`;
+//   2. (admission thread) first-in first-out: a job is admitted while the
 //      device bytes of the running jobs plus its own stay within the budget and
-//      fewer than max_active run; its session allocates from the server's pool
-//      and its projections start copying on `us`;
-//   3. a round: every running job whose projections have arrived takes one
-//      step (round 0: log/means, filter, WBP; round r: reproject, residual
-//      filter, SIRT update) and all back-projections of the round go into one
-//      persistent launch (batch_bp).  A job that took its last step gets its
-//      output transform and statistics on `cs`, then its copy-out on `ds`.
-//      At most two rounds are queued ahead of the device.
+//      fewer than max_active run; a job that does not fit yet may be passed by
+//      later ones for at most kMaxBypassMs, then it holds the line.  Its session
+//      allocates from the server's pool and its projections copy in on `us`;
+//   3. (device thread) a round: every running job whose projections have
+//      arrived takes one step (round 0: log/means, filter, WBP; round r:
+//      reproject, residual filter, SIRT update) and all back-projections of the
+//      round go into one persistent launch (batch_bp).  A job that took its last
+//      step gets its output transform and statistics on `cs`, then its copy-out
+//      on `ds`.  At most two rounds are queued ahead of the device.
 // A job's arithmetic is the same as tg_reconstruct on its own (the batched
 // back-projection is bit-identical per tile), so results do not depend on
 // the mix.
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <deque>
 #include <map>
 #include <memory>
@@ -53,10 +56,15 @@ struct SJob {
   cudaEvent_t ev_up = nullptr, ev_fin = nullptr, ev_dl = nullptr;
   int slot = -1;
   double t_submit = -1, t_admit = -1, t_done = -1, updates = 0;
+  int oom_retries = 0;
+  double retry_at = 0;  // server clock before which an OOM-requeued job is not retried
   tg_stats stats{};
+  std::string message;  // why a failed job failed
 };
 
-constexpr int kSlotBytes = 32;  // 3 floats of statistics, then the 4-int device error word
+constexpr int kSlotBytes = 32;           // 3 floats of statistics, then the 4-int device error word
+constexpr double kMaxBypassMs = 2000.0;  // how long a waiting job may be passed by later ones
+constexpr int kMaxOomRetries = 50;       // admissions retried after a device allocation failure
 
 }  // namespace
 
@@ -66,23 +74,28 @@ struct tg_server {
   int max_active = 64;
   std::chrono::steady_clock::time_point t0;
   std::mutex mu;
-  std::condition_variable cv_done;
+  std::condition_variable cv_done, cv_admit;
   std::map<uint64_t, std::shared_ptr<SJob>> jobs;
   std::deque<std::shared_ptr<SJob>> pending;
-  std::vector<std::shared_ptr<SJob>> active;  // device thread only
+  std::deque<std::shared_ptr<SJob>> admitted;   // created and copying in; the device thread takes them
+  std::vector<std::shared_ptr<SJob>> active;    // device thread only
+  int n_running = 0;                            // admitted and not yet ended
   uint64_t next_id = 1;
-  bool stop = false;
-  std::thread th;
-  cudaStream_t cs = nullptr, us = nullptr, ds = nullptr;
+  bool stop = false, admit_done = false;
+  std::thread th, th_admit;
+  cudaStream_t cs = nullptr, us = nullptr, ds = nullptr, fs = nullptr;
   cudaMemPool_t pool = nullptr;
   tg_batch batch;
   unsigned char *h_slots = nullptr;
-  std::vector<int> free_slots;
-  std::deque<cudaEvent_t> rounds_in_flight, event_pool;
+  std::vector<int> free_slots;                  // guarded by mu
+  std::mutex ev_mu;                             // guards event_pool
+  std::deque<cudaEvent_t> event_pool;
+  std::deque<std::pair<cudaEvent_t, cudaEvent_t>> rounds_in_flight;  // device thread only
+  std::vector<cudaEvent_t> timing_pool;                              // device thread only
   // counters (guarded by mu)
-  uint64_t submitted = 0, completed = 0, failed = 0, rounds = 0, bp_launches = 0;
+  uint64_t submitted = 0, completed = 0, failed = 0, rounds = 0, bp_launches = 0, oom_requeues = 0;
   size_t used = 0, peak = 0;
-  double updates_done = 0;
+  double updates_done = 0, gpu_round_ms = 0, host_round_ms = 0, host_admit_ms = 0;
   int inject_alloc = 0, inject_admit = 0;
 
   double now_ms() const {
@@ -92,11 +105,18 @@ struct tg_server {
 
 namespace {
 
+double host_ms(std::chrono::steady_clock::time_point t) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+}
+
 cudaEvent_t take_event(tg_server *sv) {
-  if (!sv->event_pool.empty()) {
-    cudaEvent_t e = sv->event_pool.back();
-    sv->event_pool.pop_back();
-    return e;
+  {
+    std::lock_guard<std::mutex> lk(sv->ev_mu);
+    if (!sv->event_pool.empty()) {
+      cudaEvent_t e = sv->event_pool.back();
+      sv->event_pool.pop_back();
+      return e;
+    }
   }
   cudaEvent_t e = nullptr;
   if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
@@ -104,31 +124,51 @@ cudaEvent_t take_event(tg_server *sv) {
 }
 
 void give_event(tg_server *sv, cudaEvent_t &e) {
-  if (e) sv->event_pool.push_back(e);
+  if (e) {
+    std::lock_guard<std::mutex> lk(sv->ev_mu);
+    sv->event_pool.push_back(e);
+  }
   e = nullptr;
 }
 
-// ends a job (called on the device thread; mu must not be held).  Its memory is
-// freed stream-ordered on ds: after its copy-out, and -- when it ends early --
-// after everything queued on cs so far, which may still use it.
+cudaEvent_t take_timing_event(tg_server *sv) {
+  if (!sv->timing_pool.empty()) {
+    cudaEvent_t e = sv->timing_pool.back();
+    sv->timing_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  return e;
+}
+
+// Ends a job (either server thread; mu must not be held).  Its memory is freed
+// on fs, a stream of its own so that frees do not queue behind other jobs'
+// copies: at once after a completed copy-out, and -- when the job ends early --
+// after everything queued so far on cs and us, which may still use it.
 void end_job(tg_server *sv, const std::shared_ptr<SJob> &j, int status) {
+  if (status != TG_OK) j->message = tg_last_error();
   if (j->s) {
     if (!j->finishing) {
-      cudaEvent_t e = take_event(sv);
-      if (e && cudaEventRecord(e, sv->cs) == cudaSuccess) cudaStreamWaitEvent(sv->ds, e, 0);
-      else cudaStreamSynchronize(sv->cs);
-      give_event(sv, e);
+      for (cudaStream_t st : {sv->cs, sv->us}) {
+        cudaEvent_t e = take_event(sv);
+        if (e && cudaEventRecord(e, st) == cudaSuccess) cudaStreamWaitEvent(sv->fs, e, 0);
+        else cudaStreamSynchronize(st);
+        give_event(sv, e);
+      }
     }
-    free_session_async(j->s, sv->ds);
+    free_session_async(j->s, sv->fs);
     j->s = nullptr;
   }
   give_event(sv, j->ev_up);
   give_event(sv, j->ev_fin);
   give_event(sv, j->ev_dl);
+  std::lock_guard<std::mutex> lk(sv->mu);
   if (j->slot >= 0) sv->free_slots.push_back(j->slot);
   j->slot = -1;
-  std::lock_guard<std::mutex> lk(sv->mu);
+  if (j->state == TG_JOB_RUNNING) --sv->n_running;
   sv->used -= j->held;
+  j->held = 0;
   j->t_done = sv->now_ms();
   j->status = status;
   j->state = status == TG_OK ? TG_JOB_DONE : TG_JOB_FAILED;
@@ -139,6 +179,15 @@ void end_job(tg_server *sv, const std::shared_ptr<SJob> &j, int status) {
     ++sv->failed;
   }
   sv->cv_done.notify_all();
+  sv->cv_admit.notify_all();
+}
+
+void drop_active(tg_server *sv, const std::shared_ptr<SJob> &j) {
+  for (size_t i = 0; i < sv->active.size(); ++i)
+    if (sv->active[i] == j) {
+      sv->active.erase(sv->active.begin() + i);
+      return;
+    }
 }
 
 // 1. finished copies
@@ -158,41 +207,89 @@ void collect(tg_server *sv) {
       j->stats.amin = f[0];
       j->stats.amax = f[1];
       j->stats.amean = f[2];
-      if (err[0]) st = (err[0] & 1) ? TG_ERR_TIMEOUT : TG_ERR_CUDA;
+      if (err[0]) {
+        set_error(err[0] & 1 ? "a bulk copy wait timed out" : "staging window outside the padded row");
+        st = (err[0] & 1) ? TG_ERR_TIMEOUT : TG_ERR_CUDA;
+      }
     }
     sv->active.erase(sv->active.begin() + i);
     end_job(sv, j, st);
   }
 }
 
-// 2. admission
-void admit(tg_server *sv) {
+// 2. admission thread: session creation overlaps the rounds
+void admit_loop(tg_server *sv) {
+  cudaSetDevice(sv->dev);
   for (;;) {
     std::shared_ptr<SJob> j;
     bool refuse = false, fail_alloc = false;
     {
-      std::lock_guard<std::mutex> lk(sv->mu);
-      if (sv->pending.empty() || (int)sv->active.size() >= sv->max_active) return;
-      j = sv->pending.front();
+      std::unique_lock<std::mutex> lk(sv->mu);
+      size_t pick = 0;
+      auto choose = [&]() {
+        if (sv->pending.empty() || sv->n_running >= sv->max_active || sv->free_slots.empty()) return false;
+        const double now = sv->now_ms();
+        for (size_t k = 0; k < sv->pending.size(); ++k) {
+          const std::shared_ptr<SJob> &c = sv->pending[k];
+          if (c->retry_at <= now && (sv->inject_admit > 0 || sv->used + c->est <= sv->budget)) {
+            pick = k;
+            return true;
+          }
+          if (now - c->t_submit > kMaxBypassMs) return false;  // it holds the line
+        }
+        return false;
+      };
+      while (!sv->stop && !choose()) sv->cv_admit.wait_for(lk, std::chrono::milliseconds(2));
+      if (sv->stop) break;
+      j = sv->pending[pick];
+      sv->pending.erase(sv->pending.begin() + pick);
       if (sv->inject_admit > 0) {
         --sv->inject_admit;
         refuse = true;
-      } else if (sv->used + j->est > sv->budget) {
-        return;  // the head waits for memory; later jobs wait behind it
+      } else {
+        if (sv->inject_alloc > 0) {
+          --sv->inject_alloc;
+          fail_alloc = true;
+        }
+        j->held = j->est;  // reserved now, corrected to the session's bytes below
+        sv->used += j->held;
+        sv->peak = std::max(sv->peak, sv->used);
+        ++sv->n_running;
+        j->slot = sv->free_slots.back();
+        sv->free_slots.pop_back();
+        j->state = TG_JOB_RUNNING;
+        j->t_admit = sv->now_ms();
       }
-      if (!refuse && sv->inject_alloc > 0) {
-        --sv->inject_alloc;
-        fail_alloc = true;
-      }
-      sv->pending.pop_front();
     }
     if (refuse) {
       set_error("admission refused (injected)");
       end_job(sv, j, TG_ERR_BUDGET);
       continue;
     }
+    const auto t_adm = std::chrono::steady_clock::now();
     tg_session *s = nullptr;
     int rc = session_create_ex(&j->g, &j->o, sv->pool, false, fail_alloc, &s);
+    if (rc == TG_ERR_OOM && !fail_alloc && j->oom_retries < kMaxOomRetries) {
+      // the budget admitted it but the pool could not map the memory yet (frees
+      // in flight, fragmentation): give unused memory back, requeue the job at
+      // the head and retry it shortly
+      (void)cudaGetLastError();
+      ++j->oom_retries;
+      cudaStreamSynchronize(sv->fs);
+      cudaMemPoolTrimTo(sv->pool, 0);
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->used -= j->held;
+      j->held = 0;
+      --sv->n_running;
+      sv->free_slots.push_back(j->slot);
+      j->slot = -1;
+      j->state = TG_JOB_QUEUED;
+      j->t_admit = -1;
+      j->retry_at = sv->now_ms() + 5.0;
+      sv->pending.push_front(j);
+      ++sv->oom_requeues;
+      continue;
+    }
     if (rc != TG_OK) {
       end_job(sv, j, rc);
       continue;
@@ -204,13 +301,11 @@ void admit(tg_server *sv) {
     j->ev_up = take_event(sv);
     j->ev_fin = take_event(sv);
     j->ev_dl = take_event(sv);
-    if (!j->ev_up || !j->ev_fin || !j->ev_dl || sv->free_slots.empty()) {
-      set_error("server out of events or result slots");
+    if (!j->ev_up || !j->ev_fin || !j->ev_dl) {
+      set_error("server out of events");
       end_job(sv, j, TG_ERR_CUDA);
       continue;
     }
-    j->slot = sv->free_slots.back();
-    sv->free_slots.pop_back();
     cudaError_t e = cudaMemcpyAsync(s->d_raw, j->h_proj, j->n * 4, cudaMemcpyHostToDevice, sv->us);
     if (e == cudaSuccess) e = cudaEventRecord(j->ev_up, sv->us);
     if (e != cudaSuccess) {
@@ -220,23 +315,30 @@ void admit(tg_server *sv) {
     s->uploaded = true;
     j->rounds_total = 1 + sirt_iters(s);
     j->updates = (double)s->onx * s->onz * s->ny * s->nviews * (1.0 + 2.0 * sirt_iters(s));
-    {
-      std::lock_guard<std::mutex> lk(sv->mu);
-      j->held = s->dev_bytes;
-      sv->used += j->held;
-      sv->peak = std::max(sv->peak, sv->used);
-      j->t_admit = sv->now_ms();
-      j->state = TG_JOB_RUNNING;
-    }
-    sv->active.push_back(j);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->used += s->dev_bytes;
+    sv->used -= j->held;
+    j->held = s->dev_bytes;
+    sv->peak = std::max(sv->peak, sv->used);
+    sv->host_admit_ms += host_ms(t_adm);
+    sv->admitted.push_back(j);
   }
+  std::lock_guard<std::mutex> lk(sv->mu);
+  sv->admit_done = true;
 }
 
 // 3. one round over every running job whose projections have arrived
 bool run_round(tg_server *sv) {
-  while (!sv->rounds_in_flight.empty() && cudaEventQuery(sv->rounds_in_flight.front()) != cudaErrorNotReady) {
-    sv->event_pool.push_back(sv->rounds_in_flight.front());
+  while (!sv->rounds_in_flight.empty() && cudaEventQuery(sv->rounds_in_flight.front().second) != cudaErrorNotReady) {
+    auto pr = sv->rounds_in_flight.front();
     sv->rounds_in_flight.pop_front();
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->gpu_round_ms += ms;
+    }
+    sv->timing_pool.push_back(pr.first);
+    sv->timing_pool.push_back(pr.second);
   }
   if (sv->rounds_in_flight.size() >= 2) return false;
   std::vector<std::shared_ptr<SJob>> ready;
@@ -246,16 +348,17 @@ bool run_round(tg_server *sv) {
     ready.push_back(j);
   }
   if (ready.empty()) return false;
+  const auto t_host = std::chrono::steady_clock::now();
+  cudaEvent_t r0 = take_timing_event(sv);
+  if (r0) cudaEventRecord(r0, sv->cs);
   std::vector<tg_session *> ss;
   std::vector<int> modes, nt;
-  std::vector<std::shared_ptr<SJob>> failed_now;
-  int launches = 0;
+  int launches = 0, rc = TG_OK;
   for (auto &j : ready) {
     tg_session *s = j->s;
-    int rc = TG_OK;
     if (j->rounds_done == 0) {
       cudaStreamWaitEvent(sv->cs, j->ev_up, 0);
-      rc = stage_front(s, &launches);
+      if (rc == TG_OK) rc = stage_front(s, &launches);
       modes.push_back(first_mode(s));
     } else {
       launch_reproject(fp_args(s), sv->cs);
@@ -263,16 +366,16 @@ bool run_round(tg_server *sv) {
       modes.push_back(2);
     }
     ss.push_back(s);
-    if (rc != TG_OK) failed_now.push_back(j);
   }
-  int rc = failed_now.empty() ? batch_bp(&sv->batch, ss, modes, nt, &launches) : TG_ERR_CUDA;
+  sv->batch.persistent_launches = 0;
+  if (rc == TG_OK) rc = batch_bp(&sv->batch, ss, modes, nt, &launches);
   if (rc != TG_OK) {  // a launch could not be issued: the round's jobs fail, the others go on
     for (auto &j : ready) {
-      for (size_t i = 0; i < sv->active.size(); ++i)
-        if (sv->active[i] == j) { sv->active.erase(sv->active.begin() + i); break; }
+      drop_active(sv, j);
       end_job(sv, j, rc);
     }
     (void)cudaGetLastError();
+    if (r0) sv->timing_pool.push_back(r0);
     return true;
   }
   for (size_t i = 0; i < ready.size(); ++i) {
@@ -293,19 +396,22 @@ bool run_round(tg_server *sv) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(slot + 16, s->d_err, 16, cudaMemcpyDeviceToHost, sv->ds);
     if (e == cudaSuccess) e = cudaEventRecord(j->ev_dl, sv->ds);
     if (e != cudaSuccess) {
-      for (size_t k = 0; k < sv->active.size(); ++k)
-        if (sv->active[k] == j) { sv->active.erase(sv->active.begin() + k); break; }
+      drop_active(sv, j);
       end_job(sv, j, rc != TG_OK ? rc : cuda_fail(e, "server finish"));
       continue;
     }
     j->finishing = true;
   }
-  cudaEvent_t re = take_event(sv);
-  if (re) {
-    cudaEventRecord(re, sv->cs);
-    sv->rounds_in_flight.push_back(re);
+  cudaEvent_t r1 = take_timing_event(sv);
+  if (r0 && r1 && cudaEventRecord(r1, sv->cs) == cudaSuccess) {
+    sv->rounds_in_flight.push_back({r0, r1});
+  } else {  // no event to bound the queue: wait for the round
+    cudaStreamSynchronize(sv->cs);
+    if (r0) sv->timing_pool.push_back(r0);
+    if (r1) sv->timing_pool.push_back(r1);
   }
   std::lock_guard<std::mutex> lk(sv->mu);
+  sv->host_round_ms += host_ms(t_host);
   ++sv->rounds;
   sv->bp_launches += sv->batch.persistent_launches;
   return true;
@@ -316,12 +422,17 @@ void device_loop(tg_server *sv) {
   for (;;) {
     {
       std::lock_guard<std::mutex> lk(sv->mu);
-      if (sv->stop) {
+      while (!sv->admitted.empty()) {
+        sv->active.push_back(sv->admitted.front());
+        sv->admitted.pop_front();
+      }
+      if (sv->stop && sv->admit_done) {
         while (!sv->pending.empty()) {  // dropped before admission
           std::shared_ptr<SJob> j = sv->pending.front();
           sv->pending.pop_front();
           j->state = TG_JOB_FAILED;
           j->status = TG_ERR_CANCELLED;
+          j->message = "cancelled by tg_server_destroy";
           j->t_done = sv->now_ms();
           ++sv->failed;
         }
@@ -330,14 +441,12 @@ void device_loop(tg_server *sv) {
       }
     }
     collect(sv);
-    admit(sv);
-    sv->batch.persistent_launches = 0;
-    bool worked = run_round(sv);
-    if (!worked) std::this_thread::sleep_for(std::chrono::microseconds(100));
+    if (!run_round(sv)) std::this_thread::sleep_for(std::chrono::microseconds(100));
   }
   cudaStreamSynchronize(sv->cs);
   cudaStreamSynchronize(sv->us);
   cudaStreamSynchronize(sv->ds);
+  cudaStreamSynchronize(sv->fs);
 }
 
 }  // namespace
@@ -371,6 +480,7 @@ int tg_server_create(int32_t device, uint64_t budget_bytes, int32_t max_active, 
   if ((e = cudaStreamCreateWithFlags(&sv->cs, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&sv->us, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&sv->ds, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&sv->fs, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaMemPoolCreate(&sv->pool, &props)) != cudaSuccess ||
       (e = cudaMemPoolSetAttribute(sv->pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess ||
       // no hidden cross-stream waits: memory is reused once its free has completed
@@ -382,6 +492,7 @@ int tg_server_create(int32_t device, uint64_t budget_bytes, int32_t max_active, 
     if (sv->cs) cudaStreamDestroy(sv->cs);
     if (sv->us) cudaStreamDestroy(sv->us);
     if (sv->ds) cudaStreamDestroy(sv->ds);
+    if (sv->fs) cudaStreamDestroy(sv->fs);
     if (sv->pool) cudaMemPoolDestroy(sv->pool);
     if (sv->batch.d_counter) cudaFree(sv->batch.d_counter);
     return rc;
@@ -391,6 +502,7 @@ int tg_server_create(int32_t device, uint64_t budget_bytes, int32_t max_active, 
   for (int i = sv->max_active - 1; i >= 0; --i) sv->free_slots.push_back(i);
   tg_server *p = sv.release();
   p->th = std::thread(device_loop, p);
+  p->th_admit = std::thread(admit_loop, p);
   *out = p;
   return TG_OK;
 }
@@ -436,6 +548,7 @@ int tg_server_submit(tg_server *sv, const tg_job *job, uint64_t *id) {
   sv->jobs[j->id] = j;
   sv->pending.push_back(j);
   ++sv->submitted;
+  sv->cv_admit.notify_all();
   *id = j->id;
   return TG_OK;
 }
@@ -451,6 +564,7 @@ static void fill_result(const SJob &j, tg_job_result *r) {
   r->updates = j.updates;
   r->device_bytes = j.held ? j.held : j.est;
   r->tag = j.tag;
+  snprintf(r->message, sizeof r->message, "%s", j.message.c_str());
 }
 
 int tg_server_poll(tg_server *sv, uint64_t id, tg_job_result *out) {
@@ -505,6 +619,10 @@ int tg_server_get_info(tg_server *sv, tg_server_info *out) {
   out->rounds = sv->rounds;
   out->bp_launches = sv->bp_launches;
   out->updates_done = sv->updates_done;
+  out->oom_requeues = sv->oom_requeues;
+  out->gpu_round_ms = sv->gpu_round_ms;
+  out->host_round_ms = sv->host_round_ms;
+  out->host_admit_ms = sv->host_admit_ms;
   return TG_OK;
 }
 
@@ -522,18 +640,24 @@ int tg_server_destroy(tg_server *sv) {
   {
     std::lock_guard<std::mutex> lk(sv->mu);
     sv->stop = true;
+    sv->cv_admit.notify_all();
   }
+  if (sv->th_admit.joinable()) sv->th_admit.join();
   if (sv->th.joinable()) sv->th.join();
   cudaSetDevice(sv->dev);
   for (cudaEvent_t e : sv->event_pool) cudaEventDestroy(e);
-  for (cudaEvent_t e : sv->rounds_in_flight) cudaEventDestroy(e);
+  for (auto &pr : sv->rounds_in_flight) {
+    cudaEventDestroy(pr.first);
+    cudaEventDestroy(pr.second);
+  }
+  for (cudaEvent_t e : sv->timing_pool) cudaEventDestroy(e);
   cudaFree(sv->batch.d_jobs);
-  cudaFree(sv->batch.d_tiles);
   cudaFree(sv->batch.d_counter);
   cudaFreeHost(sv->h_slots);
   cudaStreamDestroy(sv->cs);
   cudaStreamDestroy(sv->us);
   cudaStreamDestroy(sv->ds);
+  cudaStreamDestroy(sv->fs);
   cudaMemPoolDestroy(sv->pool);
   delete sv;
   return TG_OK;

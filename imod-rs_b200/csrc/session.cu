@@ -488,9 +488,9 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
     return TG_ERR_NO_DEVICE;
   }
   if (opt->device < 0 || opt->device >= ndev) { set_error("bad device ordinal"); return TG_ERR_INVALID_ARG; }
-  cudaDeviceProp prop;
-  TG_CUDA(cudaGetDeviceProperties(&prop, opt->device));
-  if (prop.major != 10) { set_error("libtiltgpu is built for sm_100a only"); return TG_ERR_NO_DEVICE; }
+  int major = 0;
+  TG_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, opt->device));
+  if (major != 10) { set_error("libtiltgpu is built for sm_100a only"); return TG_ERR_NO_DEVICE; }
   TG_CUDA(cudaSetDevice(opt->device));
 
   tg_session *s = new tg_session();
@@ -656,13 +656,16 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
       h[m] = (float)(acc / s->nx);
     }
     if ((rc = dalloc(s, &s->d_conv, (size_t)s->nx * 4))) return fail(rc);
-    if ((ce = cudaMemcpy(s->d_conv, h.data(), h.size() * 4, cudaMemcpyHostToDevice))) return fail(cuda_fail(ce, "copy"));
+    if ((ce = cudaMemcpyAsync(s->d_conv, h.data(), h.size() * 4, cudaMemcpyHostToDevice, s->st)))
+      return fail(cuda_fail(ce, "copy"));
   }
-  if ((ce = cudaMemcpy(s->d_weights, wt.data(), wt.size() * 4, cudaMemcpyHostToDevice)) ||
-      (ce = cudaMemcpy(s->d_tw, tw.data(), tw.size() * 8, cudaMemcpyHostToDevice)) ||
-      (ce = cudaMemcpy(s->d_vg, vg.data(), vg.size() * 16, cudaMemcpyHostToDevice)) ||
-      (ce = cudaMemcpy(s->d_vg2, vg2.data(), vg2.size() * 16, cudaMemcpyHostToDevice)) ||
-      (ce = cudaMemcpy(s->d_stretch, stretch.data(), stretch.size() * 4, cudaMemcpyHostToDevice)))
+  // on the session's stream (after its stream-ordered allocations); pageable
+  // sources have been staged when each call returns; synchronised below
+  if ((ce = cudaMemcpyAsync(s->d_weights, wt.data(), wt.size() * 4, cudaMemcpyHostToDevice, s->st)) ||
+      (ce = cudaMemcpyAsync(s->d_tw, tw.data(), tw.size() * 8, cudaMemcpyHostToDevice, s->st)) ||
+      (ce = cudaMemcpyAsync(s->d_vg, vg.data(), vg.size() * 16, cudaMemcpyHostToDevice, s->st)) ||
+      (ce = cudaMemcpyAsync(s->d_vg2, vg2.data(), vg2.size() * 16, cudaMemcpyHostToDevice, s->st)) ||
+      (ce = cudaMemcpyAsync(s->d_stretch, stretch.data(), stretch.size() * 4, cudaMemcpyHostToDevice, s->st)))
     return fail(cuda_fail(ce, "cudaMemcpy(setup)"));
   if (!any_stretch) {
     if (pool) cudaFreeAsync(s->d_stretch, s->st);

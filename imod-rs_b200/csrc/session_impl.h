@@ -86,8 +86,6 @@ struct tg_batch {
   std::vector<tg_session *> sess;
   tg::BpArgs *d_jobs = nullptr;
   size_t jobs_cap = 0;
-  int4 *d_tiles = nullptr;
-  size_t tiles_cap = 0;
   int *d_counter = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   tg_run_info info{};

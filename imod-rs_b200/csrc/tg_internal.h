@@ -86,11 +86,15 @@ struct BpArgs {
   int has_local;
   LocalDev loc;
   int nbx, ntiles_xz;       // tile grid of the fast kernel (set by its launcher)
+  int tile0;                // batched launch: index of this series' first tile
 };
-// A persistent back-projection launch over the tiles of several series.
+// A persistent back-projection launch over the tiles of several series.  Tile t
+// belongs to the series j with jobs[j].tile0 <= t < jobs[j+1].tile0 (series in
+// queue order, longest first); inside a series tiles run x fastest, then z,
+// then the row group.
 struct BatchLaunch {
-  const BpArgs *jobs;       // device array of per-series arguments (nbx, ntiles_xz filled)
-  const int4 *tiles;        // device array of (job, bx, by, bz), longest series first
+  const BpArgs *jobs;       // device array of per-series arguments (nbx, ntiles_xz, tile0 filled)
+  int njobs;
   int ntiles;
   int *counter;             // device int, reset by the launcher
   int max_views;

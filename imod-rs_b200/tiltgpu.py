@@ -77,14 +77,17 @@ class Job(C.Structure):
 class JobResult(C.Structure):
     _fields_ = [("state", _i32), ("status", _i32), ("stats", Stats), ("rounds", _i32),
                 ("submit_ms", C.c_double), ("admit_ms", C.c_double), ("done_ms", C.c_double),
-                ("updates", C.c_double), ("device_bytes", C.c_uint64), ("tag", C.c_uint64)]
+                ("updates", C.c_double), ("device_bytes", C.c_uint64), ("tag", C.c_uint64),
+                ("message", C.c_char * 128)]
 
 
 class ServerInfo(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("queued", C.c_uint64), ("running", C.c_uint64), ("budget_bytes", C.c_uint64),
                 ("bytes_in_use", C.c_uint64), ("bytes_peak", C.c_uint64), ("rounds", C.c_uint64),
-                ("bp_launches", C.c_uint64), ("updates_done", C.c_double)]
+                ("bp_launches", C.c_uint64), ("updates_done", C.c_double),
+                ("oom_requeues", C.c_uint64), ("gpu_round_ms", C.c_double),
+                ("host_round_ms", C.c_double), ("host_admit_ms", C.c_double)]
 
 
 JOB_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
@@ -384,7 +387,7 @@ def _result(r: JobResult):
             "stats": {"amin": r.stats.amin, "amax": r.stats.amax, "amean": r.stats.amean},
             "rounds": r.rounds, "submit_ms": r.submit_ms, "admit_ms": r.admit_ms,
             "done_ms": r.done_ms, "updates": r.updates, "device_bytes": r.device_bytes,
-            "tag": r.tag}
+            "tag": r.tag, "message": r.message.decode(errors="replace")}
 
 
 class Server:

@@ -163,7 +163,8 @@ int tg_batch_destroy(tg_batch *b);
  * reference, which reconstructs one series per process) ----
  * Jobs (WBP or SIRT, any size) are submitted from any thread.  One device
  * thread per server admits them first-in first-out while the device bytes of the
- * admitted jobs stay within the budget and fewer than max_active run, copies
+ * admitted jobs stay within the budget and fewer than max_active run (a job that
+ * does not fit yet may be passed by later ones for at most 2 s), copies
  * their projections in on a copy stream, and runs rounds: every round takes each
  * running job one step further (its filter + WBP pass, or one SIRT
  * reproject/residual/update) with the back-projections of all those jobs in one
@@ -192,12 +193,17 @@ typedef struct {
   double updates;           /* voxel-view updates of the job */
   uint64_t device_bytes;    /* device memory the job held while running */
   uint64_t tag;
+  char message[128];        /* why a failed job failed (empty otherwise) */
 } tg_job_result;
 typedef struct {
   uint64_t submitted, completed, failed, queued, running;
   uint64_t budget_bytes, bytes_in_use, bytes_peak;
   uint64_t rounds, bp_launches;
   double updates_done;
+  uint64_t oom_requeues;    /* admissions put back after a device allocation failure */
+  double gpu_round_ms;      /* device time of the completed rounds */
+  double host_round_ms;     /* server time spent issuing rounds */
+  double host_admit_ms;     /* server time spent creating the sessions of admitted jobs */
 } tg_server_info;
 typedef enum {
   TG_FAULT_ALLOC = 1,  /* the next `count` admissions fail their device allocation (TG_ERR_OOM) */
