@@ -8,6 +8,8 @@
 // atomics; each bin's sum is formed by one thread in a fixed order.  Without
 // x-tilt/local alignment the order (oz ascending, ox ascending) is the
 // reference's own order, so the result is bit-identical to the serial splat.
+#include <cuda_fp16.h>
+
 #include "tg_internal.h"
 #include "local_dev.cuh"
 
@@ -237,6 +239,147 @@ __global__ void interleave_kernel(const float *__restrict__ vol, float *__restri
   for (int k = 0; k < G / 4; ++k) o[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
 }
 
+// ---- half-precision reprojection (FP16/BF16 staging forms) ----
+// The volume is copied into the row-group-interleaved layout as FP16 scaled by a
+// power of two 2^(14-e), where max|v| < 2^e, so the largest value stays below
+// 2^14 and no value overflows; the scale is exact and undone on the sums.  A
+// column visit then loads S halves in S/8 16-byte loads, forms the products
+// with packed half multiplies and accumulates them in FP32 (mixed-precision
+// add).  Tolerance path: each volume value and product carries a relative
+// rounding of 2^-11 and the accumulation stays FP32.
+
+__device__ __forceinline__ void acc2_f16(float &a0, float &a1, uint32_t h2) {
+  asm("{\n .reg .f16 lo, hi;\n mov.b32 {lo, hi}, %2;\n"
+      " add.rn.f32.f16 %0, lo, %0;\n add.rn.f32.f16 %1, hi, %1;\n}\n"
+      : "+f"(a0), "+f"(a1)
+      : "r"(h2));
+}
+
+__device__ __forceinline__ float half_scale(const unsigned *maxbits, bool inverse) {
+  const float m = __uint_as_float(*maxbits);
+  if (!(m > 0.0f) || !(m < 3.0e38f)) return 1.0f;
+  int e;
+  frexpf(m, &e);  // m < 2^e
+  return inverse ? ldexpf(1.0f, e - 14) : ldexpf(1.0f, 14 - e);
+}
+
+__global__ void absmax_kernel(const float *__restrict__ vol, size_t n, unsigned *maxbits) {
+  float m = 0.0f;
+  const size_t n4 = n / 4, stride = (size_t)gridDim.x * blockDim.x;
+  const float4 *v4 = reinterpret_cast<const float4 *>(vol);  // cudaMalloc'd: 16-byte aligned
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < n4; i += 4 * stride) {  // four independent 16-byte loads in flight
+    const float4 a = __ldg(v4 + i), b = __ldg(v4 + i + stride), c = __ldg(v4 + i + 2 * stride),
+                 d = __ldg(v4 + i + 3 * stride);
+    m = fmaxf(m, fmaxf(fmaxf(fmaxf(fabsf(a.x), fabsf(a.y)), fmaxf(fabsf(a.z), fabsf(a.w))),
+                       fmaxf(fmaxf(fabsf(b.x), fabsf(b.y)), fmaxf(fabsf(b.z), fabsf(b.w)))));
+    m = fmaxf(m, fmaxf(fmaxf(fmaxf(fabsf(c.x), fabsf(c.y)), fmaxf(fabsf(c.z), fabsf(c.w))),
+                       fmaxf(fmaxf(fabsf(d.x), fabsf(d.y)), fmaxf(fabsf(d.z), fabsf(d.w)))));
+  }
+  for (; i < n4; i += stride) {
+    const float4 a = __ldg(v4 + i);
+    m = fmaxf(m, fmaxf(fmaxf(fabsf(a.x), fabsf(a.y)), fmaxf(fabsf(a.z), fabsf(a.w))));
+  }
+  if (blockIdx.x == 0 && threadIdx.x < n - 4 * n4) m = fmaxf(m, fabsf(__ldg(vol + 4 * n4 + threadIdx.x)));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(maxbits, __float_as_uint(m));  // |v| orders as its bits
+}
+
+// volh[g][oz][ox][j] = half(vol[g*G + j][oz][ox] * scale) (zero past ny)
+template <int G>
+__global__ void interleave_half_kernel(const float *__restrict__ vol, __half *__restrict__ volh, int ny,
+                                       int onz, int onx, size_t n, const unsigned *maxbits) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (g, oz, ox)
+  if (i >= n) return;
+  const float sc = half_scale(maxbits, false);
+  const size_t sl = (size_t)onz * onx;
+  const size_t g = i / sl, rem = i - g * sl;
+  uint32_t w[G / 2];
+#pragma unroll
+  for (int j = 0; j < G; j += 2) {
+    const size_t iy = g * G + j;
+    const float v0 = iy < (size_t)ny ? __ldg(vol + iy * sl + rem) * sc : 0.0f;
+    const float v1 = iy + 1 < (size_t)ny ? __ldg(vol + (iy + 1) * sl + rem) * sc : 0.0f;
+    const __half2 h = __floats2half2_rn(v0, v1);
+    w[j / 2] = *reinterpret_cast<const uint32_t *>(&h);
+  }
+  uint4 *o = reinterpret_cast<uint4 *>(volh) + i * (G / 8);
+#pragma unroll
+  for (int k = 0; k < G / 8; ++k) o[k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
+}
+
+template <int S>
+__global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
+  const int v = blockIdx.x;
+  const int p = blockIdx.y * blockDim.x + threadIdx.x;
+  const int r0 = blockIdx.z * S;
+  if (p >= a.nx) return;
+  const int nrows = min(S, a.ny - r0);
+  if (v >= a.nviews) {  // views without a tilt angle contribute nothing (main.rs:683-686)
+    for (int s = 0; s < nrows; ++s) a.sino[((size_t)v * a.ny + r0 + s) * a.nx + p] = 0.0f;
+    return;
+  }
+  const float4 g = __ldg(&a.vg[v]);
+  const float cos_t = g.x, sin_t = g.y, zf = g.z;
+  const float inv_a = 1.0f / cos_t;
+  const float lo_t = (float)(p - 1), hi_t = (float)(p + 1);
+  float acc[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) acc[s] = 0.0f;
+  auto X = [&](int ox, float t2) {
+    const float dx = __fsub_rn((float)ox, a.ocx);
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, cos_t), t2), a.cx);
+  };
+  const uint4 *vg = reinterpret_cast<const uint4 *>(a.volh) + (size_t)blockIdx.z * a.onz * a.onx * (S / 8);
+  for (int oz = 0; oz < a.onz; ++oz) {
+    const float dz = __fsub_rn((float)oz, a.cz);
+    const float t2 = __fmul_rn(__fmul_rn(dz, sin_t), zf);
+    int lo = (int)floorf((lo_t - a.cx - t2) * inv_a + a.ocx) - 1;
+    lo = min(max(lo, 0), a.onx);
+    while (lo > 0 && X(lo - 1, t2) >= lo_t) --lo;
+    while (lo < a.onx && X(lo, t2) < lo_t) ++lo;
+    const uint4 *vz = vg + (size_t)oz * a.onx * (S / 8);
+    for (int ox = lo; ox < a.onx; ++ox) {
+      const float x = X(ox, t2);
+      if (!(x < hi_t)) break;
+      const float tt = __fadd_rd(x, FMAGIC);
+      const int x0 = (int)(__float_as_uint(tt) - FMAGIC_BITS);
+      if ((unsigned)x0 > (unsigned)(a.nx - 2)) continue;
+      const float frac = __fsub_rn(x, __fsub_rn(tt, FMAGIC));
+      const __half2 w2 = __float2half2_rn(x0 == p ? __fsub_rn(1.0f, frac) : frac);
+      const uint4 *q = vz + (size_t)ox * (S / 8);
+#pragma unroll
+      for (int k = 0; k < S / 8; ++k) {
+        const uint4 u = __ldg(q + k);
+        const uint32_t uu[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const __half2 prod = __hmul2(*reinterpret_cast<const __half2 *>(&uu[m]), w2);
+          acc2_f16(acc[8 * k + 2 * m], acc[8 * k + 2 * m + 1], *reinterpret_cast<const uint32_t *>(&prod));
+        }
+      }
+    }
+  }
+  const float inv = half_scale(a.maxbits, true);
+#pragma unroll
+  for (int s = 0; s < S; ++s)
+    if (s < nrows) a.sino[((size_t)v * a.ny + r0 + s) * a.nx + p] = acc[s] * inv;
+}
+
+int fp_half_rows(int variant) { return (variant & 4) ? 32 : 16; }
+
+template <int S>
+static void launch_half(const FpArgs &a, cudaStream_t st) {
+  const size_t nvol = (size_t)a.ny * a.onz * a.onx;
+  cudaMemsetAsync(a.maxbits, 0, sizeof(unsigned), st);
+  absmax_kernel<<<8 * 148, 256, 0, st>>>(a.vol, nvol, a.maxbits);
+  const size_t n = (size_t)((a.ny + S - 1) / S) * a.onz * a.onx;
+  interleave_half_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.vol, (__half *)a.volh, a.ny, a.onz,
+                                                                         a.onx, n, a.maxbits);
+  dim3 grid(a.nviews_all, (a.nx + 127) / 128, (a.ny + S - 1) / S);
+  fp_half_kernel<S><<<grid, 128, 0, st>>>(a);
+}
+
 template <int S>
 static void launch_fast(const FpArgs &a, cudaStream_t st) {
   dim3 grid(a.nviews_all, (a.nx + 127) / 128, (a.ny + S - 1) / S);
@@ -254,6 +397,11 @@ static void launch_fast(const FpArgs &a, cudaStream_t st) {
 int fp_group_rows(int variant) { return variant == 1 || variant == 3 ? 16 : 8; }
 
 void launch_reproject(const FpArgs &a, cudaStream_t st) {
+  if (a.fast == 1 && a.volh) {
+    if (fp_half_rows(a.variant) == 32) launch_half<32>(a, st);
+    else launch_half<16>(a, st);
+    return;
+  }
   if (a.fast) {
     if (fp_group_rows(a.variant) == 16) launch_fast<16>(a, st);
     else launch_fast<8>(a, st);

@@ -142,7 +142,7 @@ static void free_session(tg_session *s) {
   }
   if (s->st) cudaStreamSynchronize(s->st);
   if (s->sirt_exec) cudaGraphExecDestroy(s->sirt_exec);
-  void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_mpart, s->d_pairs,
+  void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_volh, s->d_maxbits, s->d_mpart, s->d_pairs,
                   s->d_part, s->d_slice_stats, s->d_stats3, s->d_vg, s->d_vg2, s->d_weights,
                   s->d_conv, s->d_stretch, s->d_tw, s->d_err, s->d_lvinfo, s->d_lgoff, s->d_lxs,
                   s->d_lys, s->d_lgdx, s->d_lgdy};
@@ -156,7 +156,7 @@ static void free_session(tg_session *s) {
 
 void free_session_async(tg_session *s, cudaStream_t after) {
   if (s->sirt_exec) cudaGraphExecDestroy(s->sirt_exec);  // freed on completion if in flight
-  void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_mpart, s->d_pairs,
+  void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_volh, s->d_maxbits, s->d_mpart, s->d_pairs,
                   s->d_part, s->d_slice_stats, s->d_stats3, s->d_vg, s->d_vg2, s->d_weights,
                   s->d_conv, s->d_stretch, s->d_tw, s->d_err, s->d_lvinfo, s->d_lgoff, s->d_lxs,
                   s->d_lys, s->d_lgdx, s->d_lgdy};
@@ -377,6 +377,8 @@ FpArgs fp_args(tg_session *s) {
   f.loc = local_dev(s);
   f.fast = s->fp_fast;
   f.volg = s->d_volg;
+  f.volh = s->d_volh;
+  f.maxbits = s->d_maxbits;
   f.variant = s->fp_variant;
   return f;
 }
@@ -623,8 +625,14 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
     return fail(rc);
   if (!opt->gpu_compat && opt->sirt_iters > 0 && (rc = dalloc(s, &s->d_sino, nproj * 4))) return fail(rc);
   if (!opt->gpu_compat && opt->fake_sirt > 0 && (rc = dalloc(s, &s->d_tmp, nvol * 4))) return fail(rc);
-  if (const char *e = getenv("TG_FP_VARIANT")) s->fp_variant = atoi(e) & 3;
-  if (!opt->gpu_compat && opt->sirt_iters > 0 && s->fp_fast == 1 && (s->fp_variant & 2)) {
+  if (const char *e = getenv("TG_FP_VARIANT")) s->fp_variant = atoi(e) & 15;
+  // half staging forms reproject from an FP16 copy unless variant bit 3 asks for FP32
+  const bool half_fp = s->store != TG_STORE_FP32 && !(s->fp_variant & 8);
+  if (!opt->gpu_compat && opt->sirt_iters > 0 && s->fp_fast == 1 && half_fp) {
+    const int G = fp_half_rows(s->fp_variant);
+    const size_t ng = (size_t)((s->ny + G - 1) / G) * G * s->onz * s->onx;
+    if ((rc = dalloc(s, &s->d_volh, ng * 2)) || (rc = dalloc(s, &s->d_maxbits, 16))) return fail(rc);
+  } else if (!opt->gpu_compat && opt->sirt_iters > 0 && s->fp_fast == 1 && (s->fp_variant & 2)) {
     const int G = fp_group_rows(s->fp_variant);
     const size_t ng = (size_t)((s->ny + G - 1) / G) * G * s->onz * s->onx;
     if ((rc = dalloc(s, &s->d_volg, ng * 4))) return fail(rc);

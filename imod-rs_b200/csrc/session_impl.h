@@ -14,8 +14,10 @@ struct tg_session {  // one tilt series resident on a device
   tg_options o{};
   bool has_local = false, fast = true, zf_any = false;
   int fp_fast = 0;  // reprojector: 0 general, 1 fast (no x-tilt), 2 fast with x-tilt
-  int fp_variant = 2;  // bit 0: 16 rows per thread, bit 1: interleaved volume copy
+  int fp_variant = 2;  // reprojector variant bits (FpArgs::variant); TG_FP_VARIANT overrides
   float *d_volg = nullptr;  // interleaved copy of the volume for the reprojector
+  void *d_volh = nullptr;   // FP16 interleaved copy (half staging forms)
+  unsigned *d_maxbits = nullptr;
   int fmt = FMT_ROWPAIR, store = TG_STORE_FP32;
   int padL = 0, PW = 0, rows_alloc = 0, variant = -1, ntiles_cap = 0;
   int dev = 0;

@@ -123,10 +123,15 @@ struct FpArgs {
   LocalDev loc;
   int fast;                 // fp_fast_kernel: 1 no x-tilt (bit-exact), 2 with x-tilt; 0 general
   float *volg;              // fast == 1: row-group interleaved copy of vol, or null
-  int variant;              // bit 0: 16 rows per thread (else 8); bit 1: interleaved copy
+  void *volh;               // fast == 1, half staging: scaled FP16 interleaved copy, or null
+  unsigned *maxbits;        // with volh: max |vol| as float bits (sets the copy's scale)
+  int variant;              // bit 0: 16 rows per thread (else 8); bit 1: interleaved copy;
+                            // bit 2: 32 rows per thread in the half path (else 16);
+                            // bit 3: FP32 reprojection also for half staging
 };
 void launch_reproject(const FpArgs &a, cudaStream_t st);
 int fp_group_rows(int variant);
+int fp_half_rows(int variant);
 
 // ---- volume operations ----
 void launch_lowpass(float *vol, float *tmp, int onx, int onz, int ny, cudaStream_t st);
