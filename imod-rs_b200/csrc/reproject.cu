@@ -192,6 +192,28 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
         const float fn = floorf(yoff);
         const int iy0 = r0 - 1 - (int)fn;  // slice of i = 0
         const float *vcol = vz + ox;
+        // When iy0 + yoff and iy0 + S + yoff are positive and share a binade (so
+        // r0 >= 8), f32 rounds every iy + yoff of the group to iy + (the same
+        // multiple of the binade's ulp) -- integers are even multiples of it there,
+        // so ties go the same way -- and all slices share one fraction and one
+        // nominal or raised floor.
+        const float s0 = __fadd_rn((float)iy0, yoff), s1 = __fadd_rn((float)(iy0 + S), yoff);
+        if (s0 > 0.0f && (__float_as_uint(s0) >> 23) == (__float_as_uint(s1) >> 23)) {
+          const float fs0 = floorf(s0);
+          const bool nominal = fs0 == (float)(r0 - 1);
+          const float syf = __fsub_rn(s0, fs0);
+          const float wa = __fsub_rn(1.0f, syf), wb = nominal ? syf : 1.0f;
+#pragma unroll
+          for (int i = 0; i <= S; ++i) {
+            const int iy = iy0 + i;
+            if (i > nrows || (unsigned)iy >= (unsigned)a.ny) continue;
+            const float c = __fmul_rn(__ldg(vcol + (size_t)iy * sstride), w);
+            if (i >= 1 && nominal)
+              acc[i - 1] = __fadd_rn(acc[i - 1], __fmul_rn(c, (i - 1 == last_s) ? 1.0f : wa));
+            if (i < nrows && !(nominal && i - 1 == last_s)) acc[i] = __fadd_rn(acc[i], __fmul_rn(c, wb));
+          }
+          continue;
+        }
 #pragma unroll
         for (int i = 0; i <= S; ++i) {
           const int iy = iy0 + i;

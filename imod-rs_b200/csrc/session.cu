@@ -302,6 +302,7 @@ FilterArgs filter_args(tg_session *s, bool residual) {
 int launch_bp(tg_session *s, int mode, int *ntiles) {
   BpArgs a = bp_args(s, mode);
   if (s->fast) return launch_bp_fast(a, s->store, s->zf_any, s->variant < 0 ? 0 : s->variant, s->st, ntiles);
+  if (s->xt_fast) return launch_bp_xtilt(a, s->store, s->st, ntiles);
   return launch_bp_general(a, s->store, s->st, ntiles);
 }
 
@@ -546,6 +547,16 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
     s->fp_fast = !ok ? 0 : xt_any ? 2 : 1;
   }
   if (s->zf_any && zsmax > 2.0f) s->fast = false;
+  if (!s->fast && !s->has_local && zsmax <= 2.0f && !getenv("TG_BP_GENERAL")) {
+    float msx = 0.0f, mext = 0.0f;
+    bool ok = true;
+    for (int i = 0; i < s->nviews; ++i) {
+      ok &= hv[i].cos_t * hv[i].cos_xt > 0.0f;
+      msx = std::max(msx, fabsf(hv[i].sin_xt));
+      mext = std::max(mext, 31.0f * fabsf(hv[i].cos_t * hv[i].cos_xt) + 15.0f * fabsf(hv[i].sin_t * hv[i].zf));
+    }
+    s->xt_fast = ok && bp_xtilt_supported(s->onx, msx, mext);
+  }
   s->fmt = s->fast ? FMT_ROWPAIR : FMT_SINGLE;
 
   // cosine stretch factors (main.rs:446-460); the reference indexes

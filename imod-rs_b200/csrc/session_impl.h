@@ -13,6 +13,7 @@ struct tg_session {  // one tilt series resident on a device
   int nx = 0, ny = 0, nz = 0, onx = 0, onz = 0, nviews = 0;
   tg_options o{};
   bool has_local = false, fast = true, zf_any = false;
+  bool xt_fast = false;  // not fast: x-tilt back-projection with staged rows instead of the general kernel
   int fp_fast = 0;  // reprojector: 0 general, 1 fast (no x-tilt), 2 fast with x-tilt
   int fp_variant = 2;  // reprojector variant bits (FpArgs::variant); TG_FP_VARIANT overrides
   float *d_volg = nullptr;  // interleaved copy of the volume for the reprojector

@@ -109,6 +109,12 @@ int bp_fast_variants();
 const char *bp_fast_variant_name(int v);
 // General kernel: x-tilt, z-factor, local alignment, SINGLE format.
 int launch_bp_general(const BpArgs &a, int store, cudaStream_t st, int *ntiles_out);
+// x-tilt back-projection with staged rows (no local alignment); same tile grid
+// and partial-stat layout as the general kernel
+int launch_bp_xtilt(const BpArgs &a, int store, cudaStream_t st, int *ntiles_out);
+// max_abs_sin_xt: over the views; max_x_extent_per_tile: max over views of
+// 31*|cos*cos_xt| + 15*|sin*zf| (a 32-column, 16-depth tile)
+bool bp_xtilt_supported(int onx, float max_abs_sin_xt, float max_x_extent_per_tile);
 int bp_fast_ntiles(const BpArgs &a, int variant);
 int bp_fast_row_align();  // slices per tile of the widest fast variant
 

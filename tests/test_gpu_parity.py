@@ -65,6 +65,27 @@ def test_backprojection_bit_exact_general_xtilt():
     np.testing.assert_array_equal(vol, ref)
 
 
+@pytest.mark.parametrize("fill", ["mean", "zero", "edge"])
+@pytest.mark.parametrize("xt,shape", [(1.5, (15, 21, 70, 75, 37)), (-8.0, (11, 17, 48, 64, 20)),
+                                      ("mixed", (13, 9, 40, 33, 50))])
+def test_backprojection_bit_exact_xtilt_staged(fill, xt, shape):
+    # x-tilt back-projection from staged rows: every row pair, edge row and fill
+    # rule as the reference's f32 arithmetic, ragged tiles in x, z and y
+    nz, ny, nx, onx, onz = shape
+    proj = random_stack(nz, ny, nx, seed=nx + onz)
+    ang = np.linspace(-62, 58, nz).astype(np.float32)
+    if xt == "mixed":
+        xtv = np.linspace(-3.0, 5.0, nz).astype(np.float32)
+        xtv[2] = 0.0
+        zf = np.linspace(0.9, 1.2, nz).astype(np.float32)
+    else:
+        xtv, zf = np.full(nz, xt, np.float32), None
+    vol, st, ref, rst = both(proj, ang, no_weight=True, no_cosine_stretch=True, fill_mode=fill,
+                             xtilt=xtv, zfactor=zf, width=onx, thickness=onz)
+    np.testing.assert_array_equal(vol, ref)
+    assert st["amin"] == rst["amin"] and st["amax"] == rst["amax"]
+
+
 def test_backprojection_bit_exact_local_alignment():
     nz, ny, nx = 9, 16, 40
     proj = random_stack(nz, ny, nx, seed=5)
