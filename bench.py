@@ -403,6 +403,60 @@ def synth_job(T, torch, j, device_only=False):
     return h
 
 
+def run_c3(args):
+    """SIRT with x-axis tilt: 61 views at -60..+60 deg in 2 deg steps, 1024x1024, x-tilt
+    1.5 deg in every view, Poisson counts (base 20000) with --log, phantom 1024x1024x400;
+    WBP start then --sirt iterations (one CUDA graph per iteration).  Forms: FP32
+    staging/residuals and BF16 staging/residuals, both accumulating in FP32."""
+    import torch
+
+    import tiltgpu as T
+    torch.cuda.set_device(0)
+    nx = ny = 1024
+    onz = 400
+    ang = np.arange(-60, 61, 2.0).astype(np.float32)
+    xt = np.full(len(ang), 1.5, np.float32)
+    n_proj = len(ang) * ny * nx
+    proj_d = torch.empty(n_proj, dtype=torch.float32, device="cuda")
+    T.synth_projections(ang, nx=nx, ny=ny, vol_nz=onz, n_ell=300, rmin=3, rmax=40, dmin=0.2, dmax=1.0,
+                        n_beads=40, bead_r=5, bead_d=5.0, noise_kind=2, noise=20000.0, xtilt_deg=1.5,
+                        seed=3, out_device_ptr=proj_d.data_ptr())
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    res, vols = {}, {}
+    forms = [f for f in ("fp32", "bf16") if f in args.forms.split(",")] or ["fp32", "bf16"]
+    for form in forms:
+        s = T.Session(nx, ny, len(ang), ang, thickness=onz, radial=(0.35, 0.035), log=True, xtilt=xt,
+                      sirt=args.sirt, storage=form)
+        s.set_stream(stream.cuda_stream)
+        s.set_device(proj_d.data_ptr(), n_proj)
+        for _ in range(args.warmup if not args.profile else 1):
+            s.reconstruct(sync=False)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            s.reconstruct(sync=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        s.synchronize()
+        info = s.last_run()
+        ms = e0.elapsed_time(e1) / args.steps
+        res[form] = {"value": info["updates"] / (ms * 1e-3), "ms_per_step": ms,
+                     "stage_ms": {k: info[k] for k in ("ms_filter", "ms_backproject", "ms_reproject")},
+                     "updates_per_step": info["updates"], "kernel": s.kernel_info()["variant_name"]}
+        if not args.profile:
+            vols[form] = s.download()[0]
+        s.close()
+    line = {"metric": METRIC, "unit": "updates/s", "n_gpus": 1, "workload":
+            f"c3: SIRT {args.sirt} iterations, x-tilt 1.5 deg, 61 views 1024x1024 -> 1024x1024x400, --log",
+            "forms": res, "steps": args.steps, "data": "synthetic seeded phantom, Poisson counts, resident in HBM"}
+    if "fp32" in vols and "bf16" in vols:
+        a, b = vols["fp32"].astype(np.float64), vols["bf16"].astype(np.float64)
+        line["bf16_rel_l2_vs_fp32"] = float(np.linalg.norm(a - b) / np.linalg.norm(a))
+    print(json.dumps(line), flush=True)
+
+
 def run_c4(args):
     """64 uneven series: one persistent launch per round (FP16 staging, FP32
     accumulation) against the plain FP32 form (one series at a time)."""
@@ -579,7 +633,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "serve"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c3", "c4", "serve"])
+    ap.add_argument("--sirt", type=int, default=20, help="c3: SIRT iterations")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
     ap.add_argument("--duration", type=float, default=120.0, help="serve: seconds of arrivals")
     ap.add_argument("--large-frac", type=float, default=0.05, help="serve: share of 2048^2 jobs")
@@ -589,10 +644,13 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="time the requested forms only (no e2e, no CPU baseline); for ncu captures")
     args = ap.parse_args()
-    if not args.profile and set(args.forms.split(",")) != {"fp32", "fp16"}:
+    if not args.profile and args.workload in WORKLOADS and set(args.forms.split(",")) != {"fp32", "fp16"}:
         ap.error("--forms other than fp32,fp16 needs --profile")
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "c3":
+        run_c3(args)
+        return
     if args.workload == "c4":
         run_c4(args)
         return
