@@ -812,6 +812,16 @@ int tg_download_slices(tg_session *s, int32_t y0, int32_t y1, float *host_out, t
   return TG_OK;
 }
 
+int tg_download_slices_async(tg_session *s, int32_t y0, int32_t y1, float *host_out) {
+  if (!s || y0 < 0 || y1 > s->ny || y0 > y1 || (!host_out && y1 > y0)) return TG_ERR_INVALID_ARG;
+  TG_CUDA(cudaSetDevice(s->dev));
+  const size_t sl = (size_t)s->onx * s->onz;
+  if (y1 > y0)
+    TG_CUDA(cudaMemcpyAsync(host_out, s->d_vol + (size_t)y0 * sl, (size_t)(y1 - y0) * sl * 4,
+                            cudaMemcpyDeviceToHost, s->st));
+  return TG_OK;
+}
+
 int tg_get_stats(tg_session *s, tg_stats *stats) {
   if (!s || !stats) return TG_ERR_INVALID_ARG;
   TG_CUDA(cudaSetDevice(s->dev));
@@ -862,7 +872,7 @@ int tg_session_destroy(tg_session *s) {
 int tg_session_kernel_info(tg_session *s, int32_t *fast, int32_t *variant, int32_t *fmt,
                            int32_t *padL, int32_t *PW) {
   if (!s) return TG_ERR_INVALID_ARG;
-  if (fast) *fast = s->fast;
+  if (fast) *fast = s->fast ? 1 : s->xt_fast ? 2 : 0;  // 2: staged x-tilt kernel, 0: general kernel
   if (variant) *variant = s->variant;
   if (fmt) *fmt = s->fmt;
   if (padL) *padL = s->padL;

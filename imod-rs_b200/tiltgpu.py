@@ -113,6 +113,7 @@ EXPORTS = {
     "tg_synchronize": (C.c_int, [_P]),
     "tg_download_slices": (C.c_int, [_P, _i32, _i32, _P, C.POINTER(Stats)]),
     "tg_get_stats": (C.c_int, [_P, C.POINTER(Stats)]),
+    "tg_download_slices_async": (C.c_int, [_P, _i32, _i32, _P]),
     "tg_volume_device": (_P, [_P]),
     "tg_session_last_run": (C.c_int, [_P, C.POINTER(RunInfo)]),
     "tg_session_dims": (C.c_int, [_P, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)]),
@@ -290,8 +291,9 @@ class Session:
         vals = [_i32() for _ in range(5)]
         check(lib().tg_session_kernel_info(self.h, *[C.byref(v) for v in vals]))
         fast, variant, fmt, padl, pw = (v.value for v in vals)
-        return {"fast": bool(fast), "variant": variant,
-                "variant_name": lib().tg_variant_name(variant).decode() if fast else "general",
+        name = {1: None, 2: "xtilt-staged"}.get(fast, "general")
+        return {"fast": fast == 1, "variant": variant,
+                "variant_name": lib().tg_variant_name(variant).decode() if fast == 1 else name,
                 "fmt": fmt, "padL": padl, "PW": pw}
 
     def set_variant(self, v: int):

@@ -126,6 +126,11 @@ int tg_synchronize(tg_session *s);
 /* Copies output slices [y0, y1) ([y][out_nz][out_nx] f32) to host memory and
  * returns the whole-volume header statistics. Synchronises the session. */
 int tg_download_slices(tg_session *s, int32_t y0, int32_t y1, float *host_out, tg_stats *stats);
+/* Queues the same copy on the session's stream and returns at once (no
+ * counterpart in the reference, which writes each slice as it is made): the
+ * caller keeps host_out alive and calls tg_synchronize before reading it.
+ * Lets one series' download overlap the next series' upload and compute. */
+int tg_download_slices_async(tg_session *s, int32_t y0, int32_t y1, float *host_out);
 int tg_get_stats(tg_session *s, tg_stats *stats);
 /* Device pointer of the resident volume [ny][out_nz][out_nx]. */
 const float *tg_volume_device(tg_session *s);
