@@ -423,8 +423,9 @@ def synth_job(T, torch, j, device_only=False):
 def run_c3(args):
     """SIRT with x-axis tilt: 61 views at -60..+60 deg in 2 deg steps, 1024x1024, x-tilt
     1.5 deg in every view, Poisson counts (base 20000) with --log, phantom 1024x1024x400;
-    WBP start then --sirt iterations (one CUDA graph per iteration).  Forms: FP32
-    staging/residuals and BF16 staging/residuals, both accumulating in FP32."""
+    WBP start then --sirt iterations (one CUDA graph per iteration).  Forms: FP32,
+    FP16 and BF16 staging of the filtered projections and residuals, all accumulating
+    in FP32."""
     import torch
 
     import tiltgpu as T
@@ -441,7 +442,7 @@ def run_c3(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     res, vols = {}, {}
-    forms = [f for f in ("fp32", "fp16", "bf16") if f in (args.forms or "fp32,bf16").split(",")]
+    forms = [f for f in ("fp32", "fp16", "bf16") if f in (args.forms or "fp32,fp16,bf16").split(",")]
     for form in forms:
         s = T.Session(nx, ny, len(ang), ang, thickness=onz, radial=(0.35, 0.035), log=True, xtilt=xt,
                       sirt=args.sirt, storage=form)
@@ -468,9 +469,12 @@ def run_c3(args):
     line = {"metric": METRIC, "unit": "updates/s", "n_gpus": 1, "workload":
             f"c3: SIRT {args.sirt} iterations, x-tilt {args.xtilt} deg, 61 views 1024x1024 -> 1024x1024x400, --log",
             "forms": res, "steps": args.steps, "data": "synthetic seeded phantom, Poisson counts, resident in HBM"}
-    if "fp32" in vols and "bf16" in vols:
-        a, b = vols["fp32"].astype(np.float64), vols["bf16"].astype(np.float64)
-        line["bf16_rel_l2_vs_fp32"] = float(np.linalg.norm(a - b) / np.linalg.norm(a))
+    if "fp32" in vols:
+        a = vols["fp32"].astype(np.float64)
+        for f in ("fp16", "bf16"):
+            if f in vols:
+                b = vols[f].astype(np.float64)
+                line[f + "_rel_l2_vs_fp32"] = float(np.linalg.norm(a - b) / np.linalg.norm(a))
     print(json.dumps(line), flush=True)
 
 

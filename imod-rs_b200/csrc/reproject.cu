@@ -192,6 +192,25 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
         const float fn = floorf(yoff);
         const int iy0 = r0 - 1 - (int)fn;  // slice of i = 0
         const float *vcol = vz + ox;
+        // IL: the sheared copy holds slice iy - floor(yoff) at row iy, so the S+1 slices
+        // of this visit are row r0-1 (last of the previous group) and the group of r0
+        float vals[S + 1];
+        if (IL) {
+          const float *u = a.volg + (((size_t)blockIdx.z * a.onz + oz) * a.onx + ox) * S;  // group of r0-1
+          vals[0] = __ldg(u + S - 1);
+          const float4 *u4 = reinterpret_cast<const float4 *>(u + (size_t)a.onz * a.onx * S);
+#pragma unroll
+          for (int k = 0; k < S / 4; ++k) {
+            const float4 q = __ldg(u4 + k);
+            vals[1 + 4 * k] = q.x;
+            vals[2 + 4 * k] = q.y;
+            vals[3 + 4 * k] = q.z;
+            vals[4 + 4 * k] = q.w;
+          }
+        }
+        auto slice_val = [&](int i, int iy) {
+          return IL ? vals[i] : __ldg(vcol + (size_t)iy * sstride);
+        };
         // When iy0 + yoff and iy0 + S + yoff are positive and share a binade (so
         // r0 >= 8), f32 rounds every iy + yoff of the group to iy + (the same
         // multiple of the binade's ulp) -- integers are even multiples of it there,
@@ -207,7 +226,7 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
           for (int i = 0; i <= S; ++i) {
             const int iy = iy0 + i;
             if (i > nrows || (unsigned)iy >= (unsigned)a.ny) continue;
-            const float c = __fmul_rn(__ldg(vcol + (size_t)iy * sstride), w);
+            const float c = __fmul_rn(slice_val(i, iy), w);
             if (i >= 1 && nominal)
               acc[i - 1] = __fadd_rn(acc[i - 1], __fmul_rn(c, (i - 1 == last_s) ? 1.0f : wa));
             if (i < nrows && !(nominal && i - 1 == last_s)) acc[i] = __fadd_rn(acc[i], __fmul_rn(c, wb));
@@ -223,7 +242,7 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
           const float fs = floorf(sy);
           const bool nominal = fs == A;
           const float syf = __fsub_rn(sy, fs);
-          const float c = __fmul_rn(__ldg(vcol + (size_t)iy * sstride), w);
+          const float c = __fmul_rn(slice_val(i, iy), w);
           // lower row A = r0-1+i -> acc[i-1]; upper row A+1 -> acc[i]
           if (i >= 1 && nominal) {
             const float wa = (i - 1 == last_s) ? 1.0f : __fsub_rn(1.0f, syf);
@@ -402,10 +421,39 @@ static void launch_half(const FpArgs &a, cudaStream_t st) {
   fp_half_kernel<S><<<grid, 128, 0, st>>>(a);
 }
 
+// Sheared interleaved copy for one x-tilt shared by all views: group g (stored
+// at g+1, group -1 first) holds, for j < G, slice g*G + j - floor(dx*sin_xt) of
+// column ox (zero outside the volume).
+template <int G>
+__global__ void shear_interleave_kernel(const float *__restrict__ vol, float *__restrict__ volu, int ny,
+                                        int onz, int onx, float ocx, float sin_xt, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (g + 1, oz, ox)
+  if (i >= n) return;
+  const size_t sl = (size_t)onz * onx;
+  const size_t gs = i / sl, rem = i - gs * sl;
+  const int ox = (int)(rem % onx);
+  const int sh = (int)floorf(__fmul_rn(__fsub_rn((float)ox, ocx), sin_xt));
+  const long base = ((long)gs - 1) * G - sh;
+  float v[G];
+#pragma unroll
+  for (int j = 0; j < G; ++j) {
+    const long iy = base + j;
+    v[j] = (iy >= 0 && iy < ny) ? __ldg(vol + (size_t)iy * sl + rem) : 0.0f;
+  }
+  float4 *o = reinterpret_cast<float4 *>(volu) + i * (G / 4);
+#pragma unroll
+  for (int k = 0; k < G / 4; ++k) o[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+}
+
 template <int S>
 static void launch_fast(const FpArgs &a, cudaStream_t st) {
   dim3 grid(a.nviews_all, (a.nx + 127) / 128, (a.ny + S - 1) / S);
-  if (a.fast == 2) {
+  if (a.fast == 2 && a.volg && S == 8) {
+    const size_t n = (size_t)((a.ny + S - 1) / S + 1) * a.onz * a.onx;
+    shear_interleave_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.vol, a.volg, a.ny, a.onz, a.onx,
+                                                                          a.ocx, a.sin_xt_common, n);
+    fp_fast_kernel<S, true, true><<<grid, 128, 0, st>>>(a);
+  } else if (a.fast == 2) {
     fp_fast_kernel<S, true, false><<<grid, 128, 0, st>>>(a);
   } else if (a.volg) {
     const size_t n = (size_t)((a.ny + S - 1) / S) * a.onz * a.onx;

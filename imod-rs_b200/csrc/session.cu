@@ -378,6 +378,7 @@ FpArgs fp_args(tg_session *s) {
   f.loc = local_dev(s);
   f.fast = s->fp_fast;
   f.volg = s->d_volg;
+  f.sin_xt_common = s->sin_xt_common;
   f.volh = s->d_volh;
   f.maxbits = s->d_maxbits;
   f.variant = s->fp_variant;
@@ -545,6 +546,9 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
       ok &= hv[i].sin_xt == 0.0f || fabsf(hv[i].sin_xt) >= 1e-5f;
     }
     s->fp_fast = !ok ? 0 : xt_any ? 2 : 1;
+    s->xt_common = s->nviews > 0;
+    for (int i = 0; i < s->nviews; ++i) s->xt_common &= hv[i].sin_xt == hv[0].sin_xt;
+    if (s->xt_common) s->sin_xt_common = hv[0].sin_xt;
   }
   if (s->zf_any && zsmax > 2.0f) s->fast = false;
   if (!s->fast && !s->has_local && zsmax <= 2.0f && !getenv("TG_BP_GENERAL")) {
@@ -643,6 +647,9 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
     const int G = fp_half_rows(s->fp_variant);
     const size_t ng = (size_t)((s->ny + G - 1) / G) * G * s->onz * s->onx;
     if ((rc = dalloc(s, &s->d_volh, ng * 2)) || (rc = dalloc(s, &s->d_maxbits, 16))) return fail(rc);
+  } else if (!opt->gpu_compat && opt->sirt_iters > 0 && s->fp_fast == 2 && s->xt_common && (s->fp_variant & 2)) {
+    const size_t ng = (size_t)((s->ny + 7) / 8 + 1) * 8 * s->onz * s->onx;  // plus the group above row 0
+    if ((rc = dalloc(s, &s->d_volg, ng * 4))) return fail(rc);
   } else if (!opt->gpu_compat && opt->sirt_iters > 0 && s->fp_fast == 1 && (s->fp_variant & 2)) {
     const int G = fp_group_rows(s->fp_variant);
     const size_t ng = (size_t)((s->ny + G - 1) / G) * G * s->onz * s->onx;

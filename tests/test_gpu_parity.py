@@ -180,6 +180,22 @@ def test_sirt_xtilt_rows_and_edges(ny):
     assert rel_l2(vol, ref) <= 1e-6
 
 
+@pytest.mark.parametrize("ny,xt", [(10, -3.0), (17, 2.0), (24, 6.5)])
+def test_sirt_common_xtilt_sheared_copy(ny, xt, monkeypatch):
+    # one x-tilt for every view: the reprojector reads a copy sheared by floor(dx*sin);
+    # same products in the same order as reading the volume directly
+    nz, nx = 12, 56
+    proj = random_stack(nz, ny, nx, seed=50 + ny)
+    ang = angles(-55, 55, 10)
+    kw = dict(sirt=2, sirt_relax=0.9, no_weight=True, no_cosine_stretch=True,
+              xtilt=np.full(nz, xt, np.float32), thickness=22, width=60)
+    vol, _, ref, _ = both(proj, ang, **kw)
+    assert rel_l2(vol, ref) <= 1e-6
+    monkeypatch.setenv("TG_FP_VARIANT", "0")  # no copy: the volume itself
+    direct, _ = T.reconstruct(proj, ang, **kw)
+    np.testing.assert_array_equal(vol, direct)
+
+
 def test_sirt_xtilt_log_fake():
     nz, ny, nx = 11, 10, 40
     proj = (smooth_stack(nz, ny, nx, seed=32) * 1000.0).astype(np.float32)
