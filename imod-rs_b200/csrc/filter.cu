@@ -13,6 +13,8 @@
 
 #include <mutex>
 
+#include <cstdlib>
+
 #include "tg_internal.h"
 
 namespace tg {
@@ -380,7 +382,236 @@ __global__ void __launch_bounds__(256) filter_kernel(FilterArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Power-of-two rows (256..4096): register-resident radix-8 Stockham FFT.
+// N/8 threads per row pair; each holds 8 complex values, so a transform of
+// 2^L points is ceil(L/3) passes with one shared-memory exchange each (the
+// generic kernel above takes one pass per factor 4).  The first forward pass
+// reads the rows from global memory, the weights are applied while the inverse
+// transform's first pass loads, and the epilogue works on the complex pairs
+// (row 2j in .x, row 2j+1 in .y) without splitting them.
+// ---------------------------------------------------------------------------
+template <bool INV> __device__ __forceinline__ void dft8(float2 *v) {
+  const float h = 0.707106781186547524400844362104849039f;  // 1/sqrt(2)
+  float2 t[4], u[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    t[j] = cadd(v[j], v[j + 4]);
+    u[j] = csub(v[j], v[j + 4]);
+  }
+  // u_j *= exp(-+2 pi i j / 8)
+  {
+    const float2 d = u[1];
+    u[1] = INV ? make_float2(h * (d.x - d.y), h * (d.x + d.y)) : make_float2(h * (d.x + d.y), h * (d.y - d.x));
+  }
+  u[2] = rot<INV>(u[2]);
+  {
+    const float2 d = u[3];
+    u[3] = INV ? make_float2(-h * (d.x + d.y), h * (d.x - d.y)) : make_float2(h * (d.y - d.x), -h * (d.x + d.y));
+  }
+  bfly<4, INV>(t, nullptr, 4);
+  bfly<4, INV>(u, nullptr, 4);
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    v[2 * m] = t[m];
+    v[2 * m + 1] = u[m];
+  }
+}
+
+template <int R, bool INV> __device__ __forceinline__ void dft_r(float2 *v) {
+  if constexpr (R == 8) dft8<INV>(v);
+  else bfly<R, INV>(v, nullptr, R);
+}
+
+// One pass of radix R = min(8, N/NS) over the values x[j] = X[t + j*N/8] held by
+// thread t; writes the Stockham outputs to Y.
+template <int N, int NS, bool INV>
+__device__ __forceinline__ void p2_pass(const float2 (&x)[8], int t, const float2 *__restrict__ tw, float2 *Y) {
+  constexpr int T = N / 8;
+  constexpr int R = (N / NS) >= 8 ? 8 : N / NS;
+  constexpr int M = 8 / R;  // butterflies per thread
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int b = t + m * T;
+    const int k = b & (NS - 1);
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = x[m + M * r];  // X[b + r*N/R]
+    if constexpr (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = __ldg(&tw[r * k * (N / (NS * R))]);
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    dft_r<R, INV>(v);
+    const int base = (b - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) Y[base + r * NS] = v[r];
+  }
+}
+
+// Passes NS = 1, 8, 64, ... of one transform; x holds the first pass's inputs.
+// Returns (through `out`) the buffer holding the natural-order result.
+template <int N, int NS, bool INV>
+__device__ __forceinline__ float2 *p2_fft(float2 (&x)[8], int t, const float2 *__restrict__ tw, float2 *A,
+                                         float2 *B) {
+  constexpr int T = N / 8;
+  p2_pass<N, NS, INV>(x, t, tw, B);
+  __syncthreads();
+  if constexpr (NS * ((N / NS) >= 8 ? 8 : N / NS) < N) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = B[t + j * T];
+    return p2_fft<N, NS * 8, INV>(x, t, tw, B, A);
+  } else {
+    return B;
+  }
+}
+
+template <int N, int FMT, int STORE>
+__global__ void __launch_bounds__(N / 8) filter_p2_kernel(FilterArgs a) {
+  extern __shared__ __align__(16) unsigned char fsm[];
+  constexpr int T = N / 8;
+  float2 *A = reinterpret_cast<float2 *>(fsm);
+  float2 *B = A + N;
+  const int t = threadIdx.x;
+  const int jp = blockIdx.x, v = blockIdx.y;
+  const int r0 = 2 * jp;
+  const bool has1 = r0 + 1 < a.ny;
+  const float *in0 = a.in + ((size_t)v * a.ny + r0) * N;
+  const float *sb0 = a.sub ? a.sub + ((size_t)v * a.ny + r0) * N : nullptr;
+  float2 x[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int k = t + j * T;
+    float x0 = __ldg(in0 + k), x1 = has1 ? __ldg(in0 + N + k) : 0.0f;
+    if (sb0) {  // SIRT residual: orig - reprojection (main.rs:933-935)
+      x0 = __fsub_rn(x0, __ldg(sb0 + k));
+      if (has1) x1 = __fsub_rn(x1, __ldg(sb0 + N + k));
+    }
+    x[j] = make_float2(x0, x1);
+  }
+  float2 *F = p2_fft<N, 1, false>(x, t, a.tw, A, B);
+  float2 *G = F == A ? B : A;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {  // x the radial weight while loading the inverse's first pass
+    const int k = t + j * T;
+    const float w = __ldg(&a.weights[k]);
+    const float2 z = F[k];
+    x[j] = make_float2(__fmul_rn(z.x, w), __fmul_rn(z.y, w));
+  }
+  // the inverse's first pass writes G (free since the forward's last barrier), not F,
+  // which other threads may still be reading above
+  const float2 *Rr = p2_fft<N, 1, true>(x, t, a.tw, F, G);
+  float2 *S = const_cast<float2 *>(Rr) == A ? B : A;
+  // scale by 1/n, then the cosine stretch of both rows at once (same source x)
+  const float inv_n = a.inv_n;
+  const float stretch = a.stretch ? a.stretch[v] : 0.0f;
+  auto sc = [&](int k) {
+    const float2 z = Rr[k];
+    return make_float2(__fmul_rn(z.x, inv_n), __fmul_rn(z.y, inv_n));
+  };
+  if (stretch != 0.0f) {
+    const float center = __fdiv_rn((float)N, 2.0f);
+    for (int k = t; k < N; k += T) {
+      const float dx = __fsub_rn((float)k, center);
+      const float src_x = __fadd_rn(__fmul_rn(dx, stretch), center);
+      const float fl = floorf(src_x);
+      const int sx0 = fl < -1.0e9f ? -1000000000 : (int)fl;
+      const float frac = __fsub_rn(src_x, fl);
+      float2 o;
+      if (a.cubic && sx0 >= 1 && sx0 + 2 < N) {
+        const float2 p0 = sc(sx0 - 1), p1 = sc(sx0), p2 = sc(sx0 + 1), p3 = sc(sx0 + 2);
+        o = make_float2(cubic1d(p0.x, p1.x, p2.x, p3.x, frac), cubic1d(p0.y, p1.y, p2.y, p3.y, frac));
+      } else if (sx0 >= 0 && sx0 + 1 < N) {
+        const float2 p0 = sc(sx0), p1 = sc(sx0 + 1);
+        const float omf = __fsub_rn(1.0f, frac);
+        o = make_float2(__fadd_rn(__fmul_rn(p0.x, omf), __fmul_rn(p1.x, frac)),
+                        __fadd_rn(__fmul_rn(p0.y, omf), __fmul_rn(p1.y, frac)));
+      } else if (sx0 >= 0 && sx0 < N) {
+        o = sc(sx0);
+      } else {
+        o = make_float2(0.0f, 0.0f);
+      }
+      S[k] = o;
+    }
+  } else {
+    for (int k = t; k < N; k += T) S[k] = sc(k);
+  }
+  __syncthreads();
+  // pack into the staging format with the reference's fill rule (main.rs:386-406)
+  const float fillv = a.fill ? a.fill[v] : 0.0f;
+  auto pair = [&](int k, float2 &lo, float2 &hi) {  // (row[k], row[k+1]) of both rows, or the fill
+    if (k >= 0 && k + 1 < N) {
+      lo = S[k];
+      hi = S[k + 1];
+    } else {
+      float2 f;
+      if (a.fill_mode == TG_FILL_ZERO) f = make_float2(0.0f, 0.0f);
+      else if (a.fill_mode == TG_FILL_EDGE) f = k < 0 ? S[0] : S[N - 1];
+      else f = make_float2(fillv, fillv);
+      lo = hi = f;
+    }
+  };
+  if (FMT == FMT_ROWPAIR) {
+    uint8_t *out = reinterpret_cast<uint8_t *>(a.out) +
+                   ((size_t)v * a.rows_alloc + jp) * (size_t)a.PW * (STORE == TG_STORE_FP32 ? 16 : 8);
+    for (int e = t; e < a.PW; e += T) {
+      float2 lo, hi;
+      pair(e - a.padL, lo, hi);
+      if (!has1) lo.y = hi.y = 0.0f;
+      if (STORE == TG_STORE_FP32) {
+        reinterpret_cast<float4 *>(out)[e] = make_float4(lo.x, lo.y, hi.x, hi.y);
+      } else {
+        uint2 w;
+        w.x = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.x, lo.y);
+        w.y = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(__fsub_rn(hi.x, lo.x), __fsub_rn(hi.y, lo.y));
+        reinterpret_cast<uint2 *>(out)[e] = w;
+      }
+    }
+  } else {
+    const int eb = STORE == TG_STORE_FP32 ? 8 : 4;
+    uint8_t *o0 = reinterpret_cast<uint8_t *>(a.out) + ((size_t)v * a.rows_alloc + r0) * (size_t)a.PW * eb;
+    uint8_t *o1 = o0 + (size_t)a.PW * eb;
+    for (int e = t; e < a.PW; e += T) {
+      float2 lo, hi;
+      pair(e - a.padL, lo, hi);
+      if (STORE == TG_STORE_FP32) {
+        reinterpret_cast<float2 *>(o0)[e] = make_float2(lo.x, hi.x);
+        if (has1) reinterpret_cast<float2 *>(o1)[e] = make_float2(lo.y, hi.y);
+      } else {
+        reinterpret_cast<uint32_t *>(o0)[e] =
+            Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.x, __fsub_rn(hi.x, lo.x));
+        if (has1)
+          reinterpret_cast<uint32_t *>(o1)[e] =
+              Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.y, __fsub_rn(hi.y, lo.y));
+      }
+    }
+  }
+}
+
+template <int N, int FMT, int STORE> static void launch_p2(const FilterArgs &a, cudaStream_t st) {
+  const size_t smem = (size_t)N * 16;
+  auto k = filter_p2_kernel<N, FMT, STORE>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k<<<dim3((a.ny + 1) / 2, a.nviews), N / 8, smem, st>>>(a);
+}
+
+template <int FMT, int STORE> static bool try_p2(const FilterArgs &a, cudaStream_t st) {
+  if (!a.weights || a.conv_h || getenv("TG_FILTER_GENERIC")) return false;
+  switch (a.nx) {
+    case 256: launch_p2<256, FMT, STORE>(a, st); return true;
+    case 512: launch_p2<512, FMT, STORE>(a, st); return true;
+    case 1024: launch_p2<1024, FMT, STORE>(a, st); return true;
+    case 2048: launch_p2<2048, FMT, STORE>(a, st); return true;
+    case 4096: launch_p2<4096, FMT, STORE>(a, st); return true;
+    default: return false;
+  }
+}
+
 template <int FMT, int STORE> static void launch_f(const FilterArgs &a, cudaStream_t st) {
+  if (try_p2<FMT, STORE>(a, st)) return;
   size_t smem = (size_t)a.nx * 16;  // two complex ping-pong buffers
   auto k = filter_kernel<FMT, STORE>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

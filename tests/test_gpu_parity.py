@@ -112,6 +112,23 @@ def test_whole_path_fp32(nx):
     assert abs(st["amean"] - rst["amean"]) <= 1e-4 * max(abs(rst["amean"]), 1e-3)
 
 
+@pytest.mark.parametrize("nx,opts", [(256, dict()), (1024, dict(cosine_interp="cubic")),
+                                     (512, dict(fill_mode="edge", max_cosine_tilt=40.0)),
+                                     (256, dict(fill_mode="zero", xtilt=1.0)),
+                                     (256, dict(sirt=2, sirt_relax=0.8))])
+def test_whole_path_fp32_radix8_rows(nx, opts):
+    # power-of-two rows take the register radix-8 FFT; rows of both parities, fills,
+    # stretch, SINGLE staging (x-tilt) and the SIRT residual
+    nz, ny = 9, 5
+    proj = smooth_stack(nz, ny, nx, seed=nx + ny)
+    ang = angles(-56, 56, 14)
+    kw = dict(opts)
+    if "xtilt" in kw:
+        kw["xtilt"] = np.full(nz, kw["xtilt"], np.float32)
+    vol, _, ref, _ = both(proj, ang, radial=(0.35, 0.035), thickness=24, **kw)
+    assert rel_l2(vol, ref) <= TOL_FP32
+
+
 @pytest.mark.parametrize("opts", [dict(cosine_interp="cubic"), dict(hamming=True, radial=(0.3, 0.0)),
                                   dict(exact_filter_size=40), dict(log=True),
                                   dict(max_cosine_tilt=30.0, fill_mode="edge"),
