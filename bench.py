@@ -239,7 +239,7 @@ def run_ours(args):
     n_out = int(np.prod(out_shape))
     host_out = [torch.empty(n_out, dtype=torch.float32, pin_memory=True) for _ in range(2)]
 
-    e2e_steps = max(2, min(args.steps, 4))
+    e2e_steps = max(2, min(args.steps, 8))
     for i in range(2):  # warm both sessions (tuning, graphs)
         T.check(L.tg_upload_projections(sess[i].h, C.c_void_p(host_in.data_ptr()), n_proj))
         T.check(L.tg_reconstruct(sess[i].h))

@@ -260,6 +260,10 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
     float x2 = ref_x<ZF>(t1h, dzl, g.y, g.z, a.cx), x3 = ref_x<ZF>(t1h, dzh, g.y, g.z, a.cx);
     float xmn = fminf(fminf(x0, x1), fminf(x2, x3)), xmx = fmaxf(fmaxf(x0, x1), fmaxf(x2, x3));
     int kmin = (int)floorf(xmn), kmax = (int)floorf(xmx);
+    if (STORE != TG_STORE_FP32) {  // the FMA positions may floor one element beyond the corners
+      kmin -= 1;
+      kmax += 1;
+    }
     if (EB == 8) kmin &= ~1;  // 16-byte aligned bulk copies
     int cnt = kmax - kmin + 1;
     if (EB == 8) cnt = (cnt + 1) & ~1;
@@ -347,13 +351,18 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
         const int v = v0 + vi;
         const float4 g = __ldg(&a.vg[v]);
         const float t1 = __fmul_rn(dx, g.x);  // (dx*cos_t)*cos_xt, cos_xt == 1 exactly here
+        // half staging (a tolerance path): one FMA per position, x within an ulp of the
+        // reference's; linear interpolation is continuous, so a floor moved by it
+        // changes the sample by at most the rounding of x
+        const float t1c = __fadd_rn(t1, a.cx);
+        const float szf = ZF ? __fmul_rn(g.y, g.z) : g.y;
         const int k0 = win_k0[v];
         // shared address of element k of this view's slot: bits(tt)*EB + adj
         const uint32_t adj = smem_u32(bufs) + (uint32_t)((b * VPS + vi) * SLOT) -
                              (MAGIC_BITS + (uint32_t)k0) * (uint32_t)EB;
 #pragma unroll
         for (int j = 0; j < K; ++j) {
-          const float x = ref_x<ZF>(t1, dz[j], g.y, g.z, a.cx);
+          const float x = STORE == TG_STORE_FP32 ? ref_x<ZF>(t1, dz[j], g.y, g.z, a.cx) : fmaf(dz[j], szf, t1c);
           const float tt = __fadd_rd(x, MAGIC);  // MAGIC + floor(x), exactly
           const float f0 = __fsub_rn(x, __fsub_rn(tt, MAGIC));
           const uint32_t bits = __float_as_uint(tt);
