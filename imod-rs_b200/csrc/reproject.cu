@@ -170,8 +170,9 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
       if ((unsigned)x0 > (unsigned)(a.nx - 2)) continue;  // px0 >= 0 && px0 + 1 < nx
       const float frac = __fsub_rn(x, __fsub_rn(tt, FMAGIC));
       const float w = x0 == p ? __fsub_rn(1.0f, frac) : frac;
-      if (!XT && IL) {
-        // interleaved copy: the S slices of this row group at (oz, ox) are contiguous
+      if (IL) {
+        // interleaved copy: the S rows of this row group at (oz, ox) are contiguous; with
+        // x-tilt each holds the row's blend of its two source slices (blend_interleave_kernel)
         const float4 *q = reinterpret_cast<const float4 *>(a.volg) +
                           (((size_t)blockIdx.z * a.onz + oz) * a.onx + ox) * (S / 4);
 #pragma unroll
@@ -192,25 +193,7 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
         const float fn = floorf(yoff);
         const int iy0 = r0 - 1 - (int)fn;  // slice of i = 0
         const float *vcol = vz + ox;
-        // IL: the sheared copy holds slice iy - floor(yoff) at row iy, so the S+1 slices
-        // of this visit are row r0-1 (last of the previous group) and the group of r0
-        float vals[S + 1];
-        if (IL) {
-          const float *u = a.volg + (((size_t)blockIdx.z * a.onz + oz) * a.onx + ox) * S;  // group of r0-1
-          vals[0] = __ldg(u + S - 1);
-          const float4 *u4 = reinterpret_cast<const float4 *>(u + (size_t)a.onz * a.onx * S);
-#pragma unroll
-          for (int k = 0; k < S / 4; ++k) {
-            const float4 q = __ldg(u4 + k);
-            vals[1 + 4 * k] = q.x;
-            vals[2 + 4 * k] = q.y;
-            vals[3 + 4 * k] = q.z;
-            vals[4 + 4 * k] = q.w;
-          }
-        }
-        auto slice_val = [&](int i, int iy) {
-          return IL ? vals[i] : __ldg(vcol + (size_t)iy * sstride);
-        };
+        auto slice_val = [&](int i, int iy) { return __ldg(vcol + (size_t)iy * sstride); };
         // When iy0 + yoff and iy0 + S + yoff are positive and share a binade (so
         // r0 >= 8), f32 rounds every iy + yoff of the group to iy + (the same
         // multiple of the binade's ulp) -- integers are even multiples of it there,
@@ -421,36 +404,61 @@ static void launch_half(const FpArgs &a, cudaStream_t st) {
   fp_half_kernel<S><<<grid, 128, 0, st>>>(a);
 }
 
-// Sheared interleaved copy for one x-tilt shared by all views: group g (stored
-// at g+1, group -1 first) holds, for j < G, slice g*G + j - floor(dx*sin_xt) of
-// column ox (zero outside the volume).
+// Blended interleaved copy for one x-tilt shared by all views.  Row r of column ox
+// receives, in the reference's forward projection (main.rs:831-896), slice
+// s1 = r - floor(yoff) with weight 1-f (1 in the one-row branch: last row or zero
+// offset) when its floor row is r, and slice s0 = s1 - 1 with weight f when its
+// floor row is r-1 (nothing when that is -1), or with weight 1 when f32 rounding
+// of s0 + yoff raised its floor to r.  Those weights depend on (slice, column)
+// only, not on the view, so the blend B[r] = v(s1)*w1 + v(s0)*w0 is formed once
+// per reprojection and the views then project B like a volume without x-tilt.
+// The products are summed in another order than the reference's (tolerance path).
 template <int G>
-__global__ void shear_interleave_kernel(const float *__restrict__ vol, float *__restrict__ volu, int ny,
+__global__ void blend_interleave_kernel(const float *__restrict__ vol, float *__restrict__ volb, int ny,
                                         int onz, int onx, float ocx, float sin_xt, size_t n) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (g + 1, oz, ox)
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (g, oz, ox)
   if (i >= n) return;
   const size_t sl = (size_t)onz * onx;
-  const size_t gs = i / sl, rem = i - gs * sl;
+  const size_t g = i / sl, rem = i - g * sl;
   const int ox = (int)(rem % onx);
-  const int sh = (int)floorf(__fmul_rn(__fsub_rn((float)ox, ocx), sin_xt));
-  const long base = ((long)gs - 1) * G - sh;
-  float v[G];
+  const float yoff = __fmul_rn(__fsub_rn((float)ox, ocx), sin_xt);
+  const float fn = floorf(yoff);
+  const int nn = (int)fn;
+  const bool two_ok = fabsf(yoff) > 1e-6f;  // the reference's two-row condition
+  float b[G];
 #pragma unroll
   for (int j = 0; j < G; ++j) {
-    const long iy = base + j;
-    v[j] = (iy >= 0 && iy < ny) ? __ldg(vol + (size_t)iy * sl + rem) : 0.0f;
+    const int r = (int)g * G + j;
+    float acc = 0.0f;
+    if (r < ny) {
+      const int s1 = r - nn, s0 = s1 - 1;
+      if (s1 >= 0 && s1 < ny) {
+        const float sy = __fadd_rn((float)s1, yoff), fs = floorf(sy);
+        if (fs == (float)r) {  // floor row r (not raised)
+          const float w1 = (r == ny - 1 || !two_ok) ? 1.0f : __fsub_rn(1.0f, __fsub_rn(sy, fs));
+          acc = __fmul_rn(__ldg(vol + (size_t)s1 * sl + rem), w1);
+        }
+      }
+      if (s0 >= 0 && s0 < ny) {
+        const float sy = __fadd_rn((float)s0, yoff), fs = floorf(sy);
+        const float v0 = __ldg(vol + (size_t)s0 * sl + rem);
+        if (fs == (float)r) acc = __fadd_rn(acc, v0);  // raised floor: weight 1
+        else if (r >= 1 && two_ok) acc = __fadd_rn(acc, __fmul_rn(v0, __fsub_rn(sy, fs)));
+      }
+    }
+    b[j] = acc;
   }
-  float4 *o = reinterpret_cast<float4 *>(volu) + i * (G / 4);
+  float4 *o = reinterpret_cast<float4 *>(volb) + i * (G / 4);
 #pragma unroll
-  for (int k = 0; k < G / 4; ++k) o[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+  for (int k = 0; k < G / 4; ++k) o[k] = make_float4(b[4 * k], b[4 * k + 1], b[4 * k + 2], b[4 * k + 3]);
 }
 
 template <int S>
 static void launch_fast(const FpArgs &a, cudaStream_t st) {
   dim3 grid(a.nviews_all, (a.nx + 127) / 128, (a.ny + S - 1) / S);
-  if (a.fast == 2 && a.volg && S == 8) {
-    const size_t n = (size_t)((a.ny + S - 1) / S + 1) * a.onz * a.onx;
-    shear_interleave_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.vol, a.volg, a.ny, a.onz, a.onx,
+  if (a.fast == 2 && a.volg) {
+    const size_t n = (size_t)((a.ny + S - 1) / S) * a.onz * a.onx;
+    blend_interleave_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.vol, a.volg, a.ny, a.onz, a.onx,
                                                                           a.ocx, a.sin_xt_common, n);
     fp_fast_kernel<S, true, true><<<grid, 128, 0, st>>>(a);
   } else if (a.fast == 2) {

@@ -648,7 +648,8 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
     const size_t ng = (size_t)((s->ny + G - 1) / G) * G * s->onz * s->onx;
     if ((rc = dalloc(s, &s->d_volh, ng * 2)) || (rc = dalloc(s, &s->d_maxbits, 16))) return fail(rc);
   } else if (!opt->gpu_compat && opt->sirt_iters > 0 && s->fp_fast == 2 && s->xt_common && (s->fp_variant & 2)) {
-    const size_t ng = (size_t)((s->ny + 7) / 8 + 1) * 8 * s->onz * s->onx;  // plus the group above row 0
+    const int G = fp_group_rows(s->fp_variant);
+    const size_t ng = (size_t)((s->ny + G - 1) / G) * G * s->onz * s->onx;
     if ((rc = dalloc(s, &s->d_volg, ng * 4))) return fail(rc);
   } else if (!opt->gpu_compat && opt->sirt_iters > 0 && s->fp_fast == 1 && (s->fp_variant & 2)) {
     const int G = fp_group_rows(s->fp_variant);

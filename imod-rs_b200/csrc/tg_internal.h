@@ -129,7 +129,7 @@ struct FpArgs {
   LocalDev loc;
   int fast;                 // fp_fast_kernel: 1 no x-tilt (bit-exact), 2 with x-tilt; 0 general
   float *volg;              // fast == 1: row-group interleaved copy of vol, or null;
-                            // fast == 2: the sheared copy (one x-tilt for all views), or null
+                            // fast == 2: the blended copy (one x-tilt for all views), or null
   float sin_xt_common;      // fast == 2 with volg: the x-tilt sine shared by every view
   void *volh;               // fast == 1, half staging: scaled FP16 interleaved copy, or null
   unsigned *maxbits;        // with volh: max |vol| as float bits (sets the copy's scale)
