@@ -308,6 +308,17 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, w, proj_d)
+    if rank == 0 and world == 1 and args.workload == "c2" and not args.no_serving:
+        # the metric's latency half: a short served stream (full run: --workload serve)
+        del proj_d
+        torch.cuda.empty_cache()
+        try:
+            sv = serve_stream(20.0, args.serve_seconds, 0.05, 150.0, 16, n_large=1)
+            line["serving"] = {k: sv[k] for k in ("workload", "jobs", "done", "failed", "latency_ms", "value",
+                                                  "device_busy_updates_per_s", "serial_plain_fp32")}
+            line["serving"]["unit"] = "updates/s"
+        except Exception as exc:  # the throughput line above stands on its own
+            line["serving"] = {"error": repr(exc)[:200]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -542,7 +553,7 @@ def run_c4(args):
     print(json.dumps(line), flush=True)
 
 
-def run_serve(args):
+def serve_stream(rate, duration, large_frac, budget_gb, pool_small, n_large=2):
     """Poisson request stream through tg_server (continuous batching, HBM admission
     budget) with p50/p99 latency; beside it the same arrivals served one at a time
     by plain FP32 sessions (each pool series timed once end to end, the arrivals
@@ -550,11 +561,11 @@ def run_serve(args):
     import torch
 
     import tiltgpu as T
-    torch.cuda.set_device(0)
     rng = np.random.default_rng(20)
-    small = c4_jobs(args.pool, seed=5)
+    small = c4_jobs(pool_small, seed=5)
     big_ang = np.arange(-60, 61, 1.0).astype(np.float32)
-    large = [dict(w=2048, nv=121, ang=big_ang, thick=800, sirt=0, seed=9000 + k, noise=0.5) for k in range(2)]
+    large = [dict(w=2048, nv=121, ang=big_ang, thick=800, sirt=0, seed=9000 + k, noise=0.5)
+             for k in range(n_large)]
     t0 = time.perf_counter()
     pool = [(j, synth_job(T, torch, j)) for j in small + large]
     torch.cuda.synchronize()
@@ -563,10 +574,10 @@ def run_serve(args):
           flush=True)
     arrivals, t = [], 0.0
     while True:
-        t += rng.exponential(1.0 / args.rate)
-        if t >= args.duration:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
             break
-        if rng.random() < args.large_frac:
+        if rng.random() < large_frac:
             k = len(small) + int(rng.integers(0, len(large)))
         else:
             k = int(rng.integers(0, len(small)))
@@ -593,7 +604,7 @@ def run_serve(args):
                 s.reconstruct()
     torch.cuda.empty_cache()
     sampler = ClockSampler(0)
-    sv = T.Server(device=0, budget_bytes=int(args.budget_gb * 1e9), max_active=64)
+    sv = T.Server(device=0, budget_bytes=int(budget_gb * 1e9), max_active=64)
     ids = []
     sampler.start()
     start = time.perf_counter()
@@ -630,9 +641,9 @@ def run_serve(args):
     arr_upd = sum(job_updates(pool[k][0]) for _, k in arrivals)
     serial_busy = sum(service[k] for _, k in arrivals)
     line = {"metric": METRIC, "value": upd / (span_ms / 1e3), "unit": "updates/s", "n_gpus": 1,
-            "workload": (f"serve: Poisson {args.rate} jobs/s for {args.duration:.0f} s, C4 sizes "
-                         f"({len(small)} seeded series) + {args.large_frac:.0%} 2048^2x121-view WBP jobs "
-                         f"(thickness 800), FP16 staging, budget {args.budget_gb:.0f} GB"),
+            "workload": (f"serve: Poisson {rate} jobs/s for {duration:.0f} s, C4 sizes "
+                         f"({len(small)} seeded series) + {large_frac:.0%} 2048^2x121-view WBP jobs "
+                         f"(thickness 800), FP16 staging, budget {budget_gb:.0f} GB"),
             "jobs": len(arrivals), "done": len(done), "failed": len(results) - len(done),
             "failures": sorted({f'{r["status"]}: {r["message"]}' for r in results if r["state"] != "done"})[:5],
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
@@ -643,13 +654,20 @@ def run_serve(args):
             "bytes_peak": info["bytes_peak"],
             "device_busy_updates_per_s": upd / max(info["gpu_round_ms"] / 1e3, 1e-9),
             "serial_plain_fp32": {"value": arr_upd / serial_busy, "unit": "updates/s",
-                                  "utilisation": serial_busy / args.duration,
+                                  "utilisation": serial_busy / duration,
                                   "latency_ms_fifo_replay": {
                                       "p50": float(np.percentile(serial_lat, 50)) * 1e3,
                                       "p99": float(np.percentile(serial_lat, 99)) * 1e3},
                                   "how": "each pool series timed once end to end (upload, reconstruct, "
                                          "download); the arrivals replayed through one FIFO server"},
             "clocks": clocks, "data": "synthetic seeded phantoms, projections from pinned host memory"}
+    return line
+
+
+def run_serve(args):
+    import torch
+    torch.cuda.set_device(0)
+    line = serve_stream(args.rate, args.duration, args.large_frac, args.budget_gb, args.pool)
     print(json.dumps(line), flush=True)
 
 
@@ -669,6 +687,9 @@ def main():
     ap.add_argument("--large-frac", type=float, default=0.05, help="serve: share of 2048^2 jobs")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM admission budget")
     ap.add_argument("--pool", type=int, default=32, help="serve: distinct seeded C4-size series")
+    ap.add_argument("--serve-seconds", type=float, default=10.0,
+                    help="default run: seconds of the short served stream reported under 'serving'")
+    ap.add_argument("--no-serving", action="store_true", help="default run: skip the short served stream")
     ap.add_argument("--forms", default=None, help="staging precisions to time (c1/c2: fp32,fp16; c3: fp32,bf16)")
     ap.add_argument("--profile", action="store_true",
                     help="time the requested forms only (no e2e, no CPU baseline); for ncu captures")
