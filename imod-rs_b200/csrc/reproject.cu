@@ -279,11 +279,13 @@ __device__ __forceinline__ void acc2_f16(float &a0, float &a1, uint32_t h2) {
       : "r"(h2));
 }
 
-__device__ __forceinline__ float half_scale(const unsigned *maxbits, bool inverse) {
+// headroom: 1 when the copied values are blends of two slices (|b| < 2 max|v|)
+__device__ __forceinline__ float half_scale(const unsigned *maxbits, bool inverse, int headroom = 0) {
   const float m = __uint_as_float(*maxbits);
   if (!(m > 0.0f) || !(m < 3.0e38f)) return 1.0f;
   int e;
   frexpf(m, &e);  // m < 2^e
+  e += headroom;
   return inverse ? ldexpf(1.0f, e - 14) : ldexpf(1.0f, 14 - e);
 }
 
@@ -332,7 +334,7 @@ __global__ void interleave_half_kernel(const float *__restrict__ vol, __half *__
   for (int k = 0; k < G / 8; ++k) o[k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
 }
 
-template <int S>
+template <int S, bool XT>
 __global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
   const int v = blockIdx.x;
   const int p = blockIdx.y * blockDim.x + threadIdx.x;
@@ -344,15 +346,16 @@ __global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
     return;
   }
   const float4 g = __ldg(&a.vg[v]);
-  const float cos_t = g.x, sin_t = g.y, zf = g.z;
-  const float inv_a = 1.0f / cos_t;
+  const float cos_t = g.x, sin_t = g.y, zf = g.z, cos_xt = XT ? g.w : 1.0f;
+  const float inv_a = 1.0f / (cos_t * cos_xt);
   const float lo_t = (float)(p - 1), hi_t = (float)(p + 1);
   float acc[S];
 #pragma unroll
   for (int s = 0; s < S; ++s) acc[s] = 0.0f;
-  auto X = [&](int ox, float t2) {
+  auto X = [&](int ox, float t2) {  // ((dx*cos)*cos_xt + t2) + cx, exactly as main.rs:842
     const float dx = __fsub_rn((float)ox, a.ocx);
-    return __fadd_rn(__fadd_rn(__fmul_rn(dx, cos_t), t2), a.cx);
+    const float t1 = XT ? __fmul_rn(__fmul_rn(dx, cos_t), cos_xt) : __fmul_rn(dx, cos_t);
+    return __fadd_rn(__fadd_rn(t1, t2), a.cx);
   };
   const uint4 *vg = reinterpret_cast<const uint4 *>(a.volh) + (size_t)blockIdx.z * a.onz * a.onx * (S / 8);
   for (int oz = 0; oz < a.onz; ++oz) {
@@ -384,7 +387,7 @@ __global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
       }
     }
   }
-  const float inv = half_scale(a.maxbits, true);
+  const float inv = half_scale(a.maxbits, true, XT ? 1 : 0);
 #pragma unroll
   for (int s = 0; s < S; ++s)
     if (s < nrows) a.sino[((size_t)v * a.ny + r0 + s) * a.nx + p] = acc[s] * inv;
@@ -392,17 +395,6 @@ __global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
 
 int fp_half_rows(int variant) { return (variant & 4) ? 32 : 16; }
 
-template <int S>
-static void launch_half(const FpArgs &a, cudaStream_t st) {
-  const size_t nvol = (size_t)a.ny * a.onz * a.onx;
-  cudaMemsetAsync(a.maxbits, 0, sizeof(unsigned), st);
-  absmax_kernel<<<8 * 148, 256, 0, st>>>(a.vol, nvol, a.maxbits);
-  const size_t n = (size_t)((a.ny + S - 1) / S) * a.onz * a.onx;
-  interleave_half_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.vol, (__half *)a.volh, a.ny, a.onz,
-                                                                         a.onx, n, a.maxbits);
-  dim3 grid(a.nviews_all, (a.nx + 127) / 128, (a.ny + S - 1) / S);
-  fp_half_kernel<S><<<grid, 128, 0, st>>>(a);
-}
 
 // Blended interleaved copy for one x-tilt shared by all views.  Row r of column ox
 // receives, in the reference's forward projection (main.rs:831-896), slice
@@ -413,6 +405,27 @@ static void launch_half(const FpArgs &a, cudaStream_t st) {
 // only, not on the view, so the blend B[r] = v(s1)*w1 + v(s0)*w0 is formed once
 // per reprojection and the views then project B like a volume without x-tilt.
 // The products are summed in another order than the reference's (tolerance path).
+__device__ __forceinline__ float blend_row(const float *__restrict__ vol, int ny, size_t sl, size_t rem, int r,
+                                          int nn, float yoff, bool two_ok) {
+  float acc = 0.0f;
+  if (r >= ny) return acc;
+  const int s1 = r - nn, s0 = s1 - 1;
+  if (s1 >= 0 && s1 < ny) {
+    const float sy = __fadd_rn((float)s1, yoff), fs = floorf(sy);
+    if (fs == (float)r) {  // floor row r (not raised)
+      const float w1 = (r == ny - 1 || !two_ok) ? 1.0f : __fsub_rn(1.0f, __fsub_rn(sy, fs));
+      acc = __fmul_rn(__ldg(vol + (size_t)s1 * sl + rem), w1);
+    }
+  }
+  if (s0 >= 0 && s0 < ny) {
+    const float sy = __fadd_rn((float)s0, yoff), fs = floorf(sy);
+    const float v0 = __ldg(vol + (size_t)s0 * sl + rem);
+    if (fs == (float)r) acc = __fadd_rn(acc, v0);  // raised floor: weight 1
+    else if (r >= 1 && two_ok) acc = __fadd_rn(acc, __fmul_rn(v0, __fsub_rn(sy, fs)));
+  }
+  return acc;
+}
+
 template <int G>
 __global__ void blend_interleave_kernel(const float *__restrict__ vol, float *__restrict__ volb, int ny,
                                         int onz, int onx, float ocx, float sin_xt, size_t n) {
@@ -422,35 +435,60 @@ __global__ void blend_interleave_kernel(const float *__restrict__ vol, float *__
   const size_t g = i / sl, rem = i - g * sl;
   const int ox = (int)(rem % onx);
   const float yoff = __fmul_rn(__fsub_rn((float)ox, ocx), sin_xt);
-  const float fn = floorf(yoff);
-  const int nn = (int)fn;
+  const int nn = (int)floorf(yoff);
   const bool two_ok = fabsf(yoff) > 1e-6f;  // the reference's two-row condition
   float b[G];
 #pragma unroll
-  for (int j = 0; j < G; ++j) {
-    const int r = (int)g * G + j;
-    float acc = 0.0f;
-    if (r < ny) {
-      const int s1 = r - nn, s0 = s1 - 1;
-      if (s1 >= 0 && s1 < ny) {
-        const float sy = __fadd_rn((float)s1, yoff), fs = floorf(sy);
-        if (fs == (float)r) {  // floor row r (not raised)
-          const float w1 = (r == ny - 1 || !two_ok) ? 1.0f : __fsub_rn(1.0f, __fsub_rn(sy, fs));
-          acc = __fmul_rn(__ldg(vol + (size_t)s1 * sl + rem), w1);
-        }
-      }
-      if (s0 >= 0 && s0 < ny) {
-        const float sy = __fadd_rn((float)s0, yoff), fs = floorf(sy);
-        const float v0 = __ldg(vol + (size_t)s0 * sl + rem);
-        if (fs == (float)r) acc = __fadd_rn(acc, v0);  // raised floor: weight 1
-        else if (r >= 1 && two_ok) acc = __fadd_rn(acc, __fmul_rn(v0, __fsub_rn(sy, fs)));
-      }
-    }
-    b[j] = acc;
-  }
+  for (int j = 0; j < G; ++j) b[j] = blend_row(vol, ny, sl, rem, (int)g * G + j, nn, yoff, two_ok);
   float4 *o = reinterpret_cast<float4 *>(volb) + i * (G / 4);
 #pragma unroll
   for (int k = 0; k < G / 4; ++k) o[k] = make_float4(b[4 * k], b[4 * k + 1], b[4 * k + 2], b[4 * k + 3]);
+}
+
+// The same blend into the scaled FP16 copy of the half-staging forms (a blend of
+// two slices is below 2 max|v|: one more bit of headroom).
+template <int G>
+__global__ void blend_interleave_half_kernel(const float *__restrict__ vol, __half *__restrict__ volh, int ny,
+                                             int onz, int onx, float ocx, float sin_xt, size_t n,
+                                             const unsigned *maxbits) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (g, oz, ox)
+  if (i >= n) return;
+  const float sc = half_scale(maxbits, false, 1);
+  const size_t sl = (size_t)onz * onx;
+  const size_t g = i / sl, rem = i - g * sl;
+  const int ox = (int)(rem % onx);
+  const float yoff = __fmul_rn(__fsub_rn((float)ox, ocx), sin_xt);
+  const int nn = (int)floorf(yoff);
+  const bool two_ok = fabsf(yoff) > 1e-6f;
+  uint32_t w[G / 2];
+#pragma unroll
+  for (int j = 0; j < G; j += 2) {
+    const int r = (int)g * G + j;
+    const __half2 h = __floats2half2_rn(blend_row(vol, ny, sl, rem, r, nn, yoff, two_ok) * sc,
+                                        blend_row(vol, ny, sl, rem, r + 1, nn, yoff, two_ok) * sc);
+    w[j / 2] = *reinterpret_cast<const uint32_t *>(&h);
+  }
+  uint4 *o = reinterpret_cast<uint4 *>(volh) + i * (G / 8);
+#pragma unroll
+  for (int k = 0; k < G / 8; ++k) o[k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
+}
+
+template <int S>
+static void launch_half(const FpArgs &a, cudaStream_t st) {
+  const size_t nvol = (size_t)a.ny * a.onz * a.onx;
+  cudaMemsetAsync(a.maxbits, 0, sizeof(unsigned), st);
+  absmax_kernel<<<8 * 148, 256, 0, st>>>(a.vol, nvol, a.maxbits);
+  const size_t n = (size_t)((a.ny + S - 1) / S) * a.onz * a.onx;
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  dim3 grid(a.nviews_all, (a.nx + 127) / 128, (a.ny + S - 1) / S);
+  if (a.fast == 2) {  // one x-tilt for all views: blended rows
+    blend_interleave_half_kernel<S><<<nb, 256, 0, st>>>(a.vol, (__half *)a.volh, a.ny, a.onz, a.onx, a.ocx,
+                                                        a.sin_xt_common, n, a.maxbits);
+    fp_half_kernel<S, true><<<grid, 128, 0, st>>>(a);
+  } else {
+    interleave_half_kernel<S><<<nb, 256, 0, st>>>(a.vol, (__half *)a.volh, a.ny, a.onz, a.onx, n, a.maxbits);
+    fp_half_kernel<S, false><<<grid, 128, 0, st>>>(a);
+  }
 }
 
 template <int S>
@@ -475,7 +513,7 @@ static void launch_fast(const FpArgs &a, cudaStream_t st) {
 int fp_group_rows(int variant) { return variant == 1 || variant == 3 ? 16 : 8; }
 
 void launch_reproject(const FpArgs &a, cudaStream_t st) {
-  if (a.fast == 1 && a.volh) {
+  if ((a.fast == 1 || a.fast == 2) && a.volh) {
     if (fp_half_rows(a.variant) == 32) launch_half<32>(a, st);
     else launch_half<16>(a, st);
     return;

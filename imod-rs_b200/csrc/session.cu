@@ -643,7 +643,8 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
   if (const char *e = getenv("TG_FP_VARIANT")) s->fp_variant = atoi(e) & 15;
   // half staging forms reproject from an FP16 copy unless variant bit 3 asks for FP32
   const bool half_fp = s->store != TG_STORE_FP32 && !(s->fp_variant & 8);
-  if (!opt->gpu_compat && opt->sirt_iters > 0 && s->fp_fast == 1 && half_fp) {
+  if (!opt->gpu_compat && opt->sirt_iters > 0 && half_fp &&
+      (s->fp_fast == 1 || (s->fp_fast == 2 && s->xt_common))) {
     const int G = fp_half_rows(s->fp_variant);
     const size_t ng = (size_t)((s->ny + G - 1) / G) * G * s->onz * s->onx;
     if ((rc = dalloc(s, &s->d_volh, ng * 2)) || (rc = dalloc(s, &s->d_maxbits, 16))) return fail(rc);

@@ -153,13 +153,16 @@ def test_half_storage_vs_fp64(storage):
 
 
 @pytest.mark.parametrize("storage", ["fp16", "bf16"])
-def test_sirt_half_storage_vs_fp64(storage):
-    # half staging forms also reproject from a scaled FP16 copy of the volume
+@pytest.mark.parametrize("xt", [0.0, 2.0])
+def test_sirt_half_storage_vs_fp64(storage, xt):
+    # half staging forms also reproject from a scaled FP16 copy of the volume (with one
+    # x-tilt for all views: of its blended rows)
     nz, ny, nx = 31, 19, 96
     proj = smooth_stack(nz, ny, nx, seed=22)
     ang = angles(-60, 60, 4)
+    kw = dict(xtilt=np.full(nz, xt, np.float32)) if xt else {}
     vol, _, ref, _ = both(proj, ang, precision="64g", storage=storage, radial=(0.35, 0.035),
-                          thickness=40, sirt=4, sirt_relax=0.8)
+                          thickness=40, sirt=4, sirt_relax=0.8, **kw)
     err = rel_l2(vol, ref)
     assert err <= (TOL_HALF if storage == "fp16" else 4 * TOL_HALF), err
 
