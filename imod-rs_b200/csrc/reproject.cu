@@ -352,15 +352,16 @@ __global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
   float acc[S];
 #pragma unroll
   for (int s = 0; s < S; ++s) acc[s] = 0.0f;
-  auto X = [&](int ox, float t2) {  // ((dx*cos)*cos_xt + t2) + cx, exactly as main.rs:842
-    const float dx = __fsub_rn((float)ox, a.ocx);
-    const float t1 = XT ? __fmul_rn(__fmul_rn(dx, cos_t), cos_xt) : __fmul_rn(dx, cos_t);
-    return __fadd_rn(__fadd_rn(t1, t2), a.cx);
-  };
+  // Tolerance path: x(ox) = ox*c + c0 with one FMA (within a few ulp of the reference's
+  // ((dx*cos)*cos_xt + t2) + cx, and non-decreasing in ox, which the search needs)
+  const float c = XT ? cos_t * cos_xt : cos_t;
+  float c0 = 0.0f;
+  auto X = [&](int ox, float) { return fmaf((float)ox, c, c0); };
   const uint4 *vg = reinterpret_cast<const uint4 *>(a.volh) + (size_t)blockIdx.z * a.onz * a.onx * (S / 8);
   for (int oz = 0; oz < a.onz; ++oz) {
     const float dz = __fsub_rn((float)oz, a.cz);
     const float t2 = __fmul_rn(__fmul_rn(dz, sin_t), zf);
+    c0 = fmaf(-a.ocx, c, t2 + a.cx);
     int lo = (int)floorf((lo_t - a.cx - t2) * inv_a + a.ocx) - 1;
     lo = min(max(lo, 0), a.onx);
     while (lo > 0 && X(lo - 1, t2) >= lo_t) --lo;
