@@ -541,6 +541,12 @@ def run_c4(args):
             b.reconstruct()
             times.append(time.perf_counter() - t0)
         res["batched_" + storage] = upd / min(times)
+        if args.profile:  # per-kernel device time of one batched run (CUPTI through torch.profiler)
+            from torch.profiler import ProfilerActivity, profile
+            with profile(activities=[ProfilerActivity.CUDA]) as prof:
+                b.reconstruct()
+            res["kernels_ms_" + storage] = {e.key[:60]: round(e.device_time_total / 1000.0, 2)
+                                            for e in prof.key_averages() if e.device_time_total > 0}
         b.close()
         for s in ss:
             s.close()
@@ -549,6 +555,7 @@ def run_c4(args):
             "plain_fp32": res["plain_fp32"], "batched_fp32": res["batched_fp32"],
             "batched_fp16_over_plain_fp32": res["batched_fp16"] / res["plain_fp32"],
             "updates_per_step": upd, "steps": args.steps, "timing": "best of steps, wall clock with sync",
+            **{k: v for k, v in res.items() if k.startswith("kernels_ms_")},
             "data": "synthetic seeded phantoms, projections resident in HBM"}
     print(json.dumps(line), flush=True)
 
