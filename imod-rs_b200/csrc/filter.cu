@@ -383,10 +383,11 @@ __global__ void __launch_bounds__(256) filter_kernel(FilterArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Power-of-two rows (256..4096): register-resident radix-8 Stockham FFT.
-// N/8 threads per row pair; each holds 8 complex values, so a transform of
-// 2^L points is ceil(L/3) passes with one shared-memory exchange each (the
-// generic kernel above takes one pass per factor 4).  The first forward pass
+// Rows of 2^k (256..4096) or 3*2^k (384..3072) samples: register-resident
+// Stockham FFT.  N/V threads per row pair, each holding V complex values (8 for
+// 2^k: radix-8 passes, a transform of 2^L points in ceil(L/3) passes; 12 or 24
+// for 3*2^k: radix 8/4/2 passes and a final radix-3 pass), one shared-memory
+// exchange per pass (the generic kernel above takes one pass per factor 4).  The first forward pass
 // reads the rows from global memory, the weights are applied while the inverse
 // transform's first pass loads, and the epilogue works on the complex pairs
 // (row 2j in .x, row 2j+1 in .y) without splitting them.
@@ -423,17 +424,25 @@ template <int R, bool INV> __device__ __forceinline__ void dft_r(float2 *v) {
   else bfly<R, INV>(v, nullptr, R);
 }
 
-// One pass of radix R = min(8, N/NS) over the values x[j] = X[t + j*N/8] held by
-// thread t; writes the Stockham outputs to Y.
-template <int N, int NS, bool INV>
-__device__ __forceinline__ void p2_pass(const float2 (&x)[8], int t, const float2 *__restrict__ tw, float2 *Y) {
-  constexpr int T = N / 8;
-  constexpr int R = (N / NS) >= 8 ? 8 : N / NS;
-  constexpr int M = 8 / R;  // butterflies per thread
+// Radix of the pass that starts at span NS, for V values per thread: 8, 4 or 2
+// while N/NS allows it (and V is a multiple), the factor 3 of 3*2^k lengths last.
+template <int N, int NS, int V> struct PassRadix {
+  static constexpr int Q = N / NS;
+  static constexpr int R = (Q % 8 == 0 && V % 8 == 0) ? 8 : (Q % 4 == 0 && V % 4 == 0) ? 4
+                           : (Q % 2 == 0 && V % 2 == 0) ? 2 : 3;
+};
+
+// One Stockham pass over the values x[j] = X[t + j*N/V] held by thread t (V per
+// thread, so a pass of radix R is V/R butterflies per thread); writes to Y.
+template <int N, int V, int NS, bool INV>
+__device__ __forceinline__ void p2_pass(const float2 (&x)[V], int t, const float2 *__restrict__ tw, float2 *Y) {
+  constexpr int T = N / V;
+  constexpr int R = PassRadix<N, NS, V>::R;
+  constexpr int M = V / R;  // butterflies per thread
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     const int b = t + m * T;
-    const int k = b & (NS - 1);
+    const int k = b % NS;
     float2 v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = x[m + M * r];  // X[b + r*N/R]
@@ -452,27 +461,28 @@ __device__ __forceinline__ void p2_pass(const float2 (&x)[8], int t, const float
   }
 }
 
-// Passes NS = 1, 8, 64, ... of one transform; x holds the first pass's inputs.
-// Returns (through `out`) the buffer holding the natural-order result.
-template <int N, int NS, bool INV>
-__device__ __forceinline__ float2 *p2_fft(float2 (&x)[8], int t, const float2 *__restrict__ tw, float2 *A,
+// The passes of one transform; x holds the first pass's inputs.  Returns the
+// buffer holding the natural-order result.
+template <int N, int V, int NS, bool INV>
+__device__ __forceinline__ float2 *p2_fft(float2 (&x)[V], int t, const float2 *__restrict__ tw, float2 *A,
                                          float2 *B) {
-  constexpr int T = N / 8;
-  p2_pass<N, NS, INV>(x, t, tw, B);
+  constexpr int T = N / V;
+  constexpr int R = PassRadix<N, NS, V>::R;
+  p2_pass<N, V, NS, INV>(x, t, tw, B);
   __syncthreads();
-  if constexpr (NS * ((N / NS) >= 8 ? 8 : N / NS) < N) {
+  if constexpr (NS * R < N) {
 #pragma unroll
-    for (int j = 0; j < 8; ++j) x[j] = B[t + j * T];
-    return p2_fft<N, NS * 8, INV>(x, t, tw, B, A);
+    for (int j = 0; j < V; ++j) x[j] = B[t + j * T];
+    return p2_fft<N, V, NS * R, INV>(x, t, tw, B, A);
   } else {
     return B;
   }
 }
 
-template <int N, int FMT, int STORE>
-__global__ void __launch_bounds__(N / 8) filter_p2_kernel(FilterArgs a) {
+template <int N, int V, int FMT, int STORE>
+__global__ void __launch_bounds__(N / V) filter_p2_kernel(FilterArgs a) {
   extern __shared__ __align__(16) unsigned char fsm[];
-  constexpr int T = N / 8;
+  constexpr int T = N / V;
   float2 *A = reinterpret_cast<float2 *>(fsm);
   float2 *B = A + N;
   const int t = threadIdx.x;
@@ -481,9 +491,9 @@ __global__ void __launch_bounds__(N / 8) filter_p2_kernel(FilterArgs a) {
   const bool has1 = r0 + 1 < a.ny;
   const float *in0 = a.in + ((size_t)v * a.ny + r0) * N;
   const float *sb0 = a.sub ? a.sub + ((size_t)v * a.ny + r0) * N : nullptr;
-  float2 x[8];
+  float2 x[V];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < V; ++j) {
     const int k = t + j * T;
     float x0 = __ldg(in0 + k), x1 = has1 ? __ldg(in0 + N + k) : 0.0f;
     if (sb0) {  // SIRT residual: orig - reprojection (main.rs:933-935)
@@ -492,10 +502,10 @@ __global__ void __launch_bounds__(N / 8) filter_p2_kernel(FilterArgs a) {
     }
     x[j] = make_float2(x0, x1);
   }
-  float2 *F = p2_fft<N, 1, false>(x, t, a.tw, A, B);
+  float2 *F = p2_fft<N, V, 1, false>(x, t, a.tw, A, B);
   float2 *G = F == A ? B : A;
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {  // x the radial weight while loading the inverse's first pass
+  for (int j = 0; j < V; ++j) {  // x the radial weight while loading the inverse's first pass
     const int k = t + j * T;
     const float w = __ldg(&a.weights[k]);
     const float2 z = F[k];
@@ -503,7 +513,7 @@ __global__ void __launch_bounds__(N / 8) filter_p2_kernel(FilterArgs a) {
   }
   // the inverse's first pass writes G (free since the forward's last barrier), not F,
   // which other threads may still be reading above
-  const float2 *Rr = p2_fft<N, 1, true>(x, t, a.tw, F, G);
+  const float2 *Rr = p2_fft<N, V, 1, true>(x, t, a.tw, F, G);
   float2 *S = const_cast<float2 *>(Rr) == A ? B : A;
   // scale by 1/n, then the cosine stretch of both rows at once (same source x)
   const float inv_n = a.inv_n;
@@ -591,21 +601,25 @@ __global__ void __launch_bounds__(N / 8) filter_p2_kernel(FilterArgs a) {
   }
 }
 
-template <int N, int FMT, int STORE> static void launch_p2(const FilterArgs &a, cudaStream_t st) {
+template <int N, int V, int FMT, int STORE> static void launch_p2(const FilterArgs &a, cudaStream_t st) {
   const size_t smem = (size_t)N * 16;
-  auto k = filter_p2_kernel<N, FMT, STORE>;
+  auto k = filter_p2_kernel<N, V, FMT, STORE>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k<<<dim3((a.ny + 1) / 2, a.nviews), N / 8, smem, st>>>(a);
+  k<<<dim3((a.ny + 1) / 2, a.nviews), N / V, smem, st>>>(a);
 }
 
 template <int FMT, int STORE> static bool try_p2(const FilterArgs &a, cudaStream_t st) {
   if (!a.weights || a.conv_h || getenv("TG_FILTER_GENERIC")) return false;
   switch (a.nx) {
-    case 256: launch_p2<256, FMT, STORE>(a, st); return true;
-    case 512: launch_p2<512, FMT, STORE>(a, st); return true;
-    case 1024: launch_p2<1024, FMT, STORE>(a, st); return true;
-    case 2048: launch_p2<2048, FMT, STORE>(a, st); return true;
-    case 4096: launch_p2<4096, FMT, STORE>(a, st); return true;
+    case 256: launch_p2<256, 8, FMT, STORE>(a, st); return true;
+    case 512: launch_p2<512, 8, FMT, STORE>(a, st); return true;
+    case 1024: launch_p2<1024, 8, FMT, STORE>(a, st); return true;
+    case 2048: launch_p2<2048, 8, FMT, STORE>(a, st); return true;
+    case 4096: launch_p2<4096, 8, FMT, STORE>(a, st); return true;
+    case 384: launch_p2<384, 12, FMT, STORE>(a, st); return true;  // 3 * 2^k: 12 or 24 values per thread
+    case 768: launch_p2<768, 24, FMT, STORE>(a, st); return true;
+    case 1536: launch_p2<1536, 24, FMT, STORE>(a, st); return true;
+    case 3072: launch_p2<3072, 24, FMT, STORE>(a, st); return true;
     default: return false;
   }
 }

@@ -113,11 +113,12 @@ def test_whole_path_fp32(nx):
 
 
 @pytest.mark.parametrize("nx,opts", [(256, dict()), (1024, dict(cosine_interp="cubic")),
+                                     (384, dict()), (768, dict(fill_mode="edge", sirt=1)),
                                      (512, dict(fill_mode="edge", max_cosine_tilt=40.0)),
                                      (256, dict(fill_mode="zero", xtilt=1.0)),
                                      (256, dict(sirt=2, sirt_relax=0.8))])
 def test_whole_path_fp32_radix8_rows(nx, opts):
-    # power-of-two rows take the register radix-8 FFT; rows of both parities, fills,
+    # 2^k and 3*2^k rows take the register-resident FFT; rows of both parities, fills,
     # stretch, SINGLE staging (x-tilt) and the SIRT residual
     nz, ny = 9, 5
     proj = smooth_stack(nz, ny, nx, seed=nx + ny)
