@@ -214,7 +214,16 @@ def run_ours(args):
         if form == "fp16":
             sess16 = s
         else:
-            s.close()
+            sess32 = s
+    # the first slices of both forms, for the accuracy check against the oracle below
+    acc_rows = 16
+    first = {}
+    for form, s_ in (("fp32", locals().get("sess32")), ("fp16", locals().get("sess16"))):
+        if s_ is not None:
+            s_.reconstruct(sync=True)
+            first[form] = s_.download(0, min(acc_rows, s_.out_shape[0]))[0].copy()
+    if "sess32" in locals():
+        sess32.close()
     if args.profile:  # small-case profiling run: stage times only
         if rank == 0:
             print(json.dumps({f: {k: r[k] for k in ("ms", "bp_ms", "filter_ms")} | {"kernel": r["kernel"]}
@@ -307,7 +316,15 @@ def run_ours(args):
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args, w, proj_d)
+        line["cpu_baseline"], ref_rows = cpu_baseline(args, w, proj_d, nslices=acc_rows, want_rows=True)
+        # error of both forms on those slices against the oracle's f32 restatement of the reference
+        line["accuracy"] = {}
+        for form, got in first.items():
+            d = got.astype(np.float64) - ref_rows.astype(np.float64)
+            line["accuracy"][form + "_vs_ref32"] = {
+                "rel_l2": float(np.linalg.norm(d) / np.linalg.norm(ref_rows.astype(np.float64))),
+                "max_abs": float(np.abs(d).max()), "ref_max_abs": float(np.abs(ref_rows).max()),
+                "slices": acc_rows}
     if rank == 0 and world == 1 and args.workload == "c2" and not args.no_serving:
         # the metric's latency half: a short served stream (full run: --workload serve)
         del proj_d
@@ -325,7 +342,7 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def cpu_baseline(args, w, proj_d=None, nslices=16):
+def cpu_baseline(args, w, proj_d=None, nslices=16, want_rows=False):
     """The oracle port (ref32, all host threads) on slices [0, nslices) of the workload."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -339,12 +356,13 @@ def cpu_baseline(args, w, proj_d=None, nslices=16):
     p = O.Params(nx, ny, nz, ang, width=onx, thickness=onz, radial=w["radial"], log=True)
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
-    O.wbp_rows(p, proj, 0, nslices, nthreads=cores)
+    rows = O.wbp_rows(p, proj, 0, nslices, nthreads=cores)
     dt = time.perf_counter() - t0
     upd = float(onx) * onz * nslices * nz
-    return {"value": upd / dt, "unit": "updates/s", "cores": cores, "kind": "port",
-            "sample": f"slices 0..{nslices} of the workload (filter of their rows + stretch + WBP), "
-                      f"{upd:.3g} updates in {dt:.2f} s"}
+    res = {"value": upd / dt, "unit": "updates/s", "cores": cores, "kind": "port",
+           "sample": f"slices 0..{nslices} of the workload (filter of their rows + stretch + WBP), "
+                     f"{upd:.3g} updates in {dt:.2f} s"}
+    return (res, rows) if want_rows else res
 
 
 def seeded_rows(nz, ny, nx, nrows, seed=5):
