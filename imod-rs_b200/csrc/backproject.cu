@@ -573,6 +573,11 @@ static const FastVariant kFast[] = {
     {16, 2, 32, 128, 2, 4, "S16K2TX32NT128V2N4"},
     {16, 2, 32, 256, 2, 4, "S16K2TX32NT256V2N4"},
     {8, 8, 32, 128, 2, 4, "S8K8TX32NT128V2N4"},
+    {8, 8, 32, 256, 2, 4, "S8K8TX32NT256V2N4"},
+    {8, 4, 32, 256, 4, 3, "S8K4TX32NT256V4N3"},
+    {8, 4, 32, 256, 8, 2, "S8K4TX32NT256V8N2"},
+    {8, 4, 32, 256, 8, 3, "S8K4TX32NT256V8N3"},
+    {8, 4, 64, 256, 4, 3, "S8K4TX64NT256V4N3"},
 };
 constexpr int MAX_S = 16;  // rows per tile of the widest variant (sizes the staging buffer)
 int bp_fast_variants() { return (int)(sizeof(kFast) / sizeof(kFast[0])); }
@@ -625,7 +630,12 @@ static int launch_fast_v(const BpArgs &a, int variant, cudaStream_t st, int *nti
     case 3: return launch_fast_t<STORE, 8, 4, 64, 256, 2, 4, ZF>(a, st, ntiles);
     case 4: return launch_fast_t<STORE, 16, 2, 32, 128, 2, 4, ZF>(a, st, ntiles);
     case 5: return launch_fast_t<STORE, 16, 2, 32, 256, 2, 4, ZF>(a, st, ntiles);
-    default: return launch_fast_t<STORE, 8, 8, 32, 128, 2, 4, ZF>(a, st, ntiles);
+    case 6: return launch_fast_t<STORE, 8, 8, 32, 128, 2, 4, ZF>(a, st, ntiles);
+    case 7: return launch_fast_t<STORE, 8, 8, 32, 256, 2, 4, ZF>(a, st, ntiles);
+    case 8: return launch_fast_t<STORE, 8, 4, 32, 256, 4, 3, ZF>(a, st, ntiles);
+    case 9: return launch_fast_t<STORE, 8, 4, 32, 256, 8, 2, ZF>(a, st, ntiles);
+    case 10: return launch_fast_t<STORE, 8, 4, 32, 256, 8, 3, ZF>(a, st, ntiles);
+    default: return launch_fast_t<STORE, 8, 4, 64, 256, 4, 3, ZF>(a, st, ntiles);
   }
 }
 
@@ -638,7 +648,12 @@ static int launch_batch_v(const BatchLaunch &bl, int variant, cudaStream_t st) {
     case 3: return launch_batch_t<STORE, 8, 4, 64, 256, 2, 4, ZF>(bl, st);
     case 4: return launch_batch_t<STORE, 16, 2, 32, 128, 2, 4, ZF>(bl, st);
     case 5: return launch_batch_t<STORE, 16, 2, 32, 256, 2, 4, ZF>(bl, st);
-    default: return launch_batch_t<STORE, 8, 8, 32, 128, 2, 4, ZF>(bl, st);
+    case 6: return launch_batch_t<STORE, 8, 8, 32, 128, 2, 4, ZF>(bl, st);
+    case 7: return launch_batch_t<STORE, 8, 8, 32, 256, 2, 4, ZF>(bl, st);
+    case 8: return launch_batch_t<STORE, 8, 4, 32, 256, 4, 3, ZF>(bl, st);
+    case 9: return launch_batch_t<STORE, 8, 4, 32, 256, 8, 2, ZF>(bl, st);
+    case 10: return launch_batch_t<STORE, 8, 4, 32, 256, 8, 3, ZF>(bl, st);
+    default: return launch_batch_t<STORE, 8, 4, 64, 256, 4, 3, ZF>(bl, st);
   }
 }
 
