@@ -719,7 +719,7 @@ __global__ void __launch_bounds__(NT) bp_general_kernel(BpArgs a) {
     const float yoff = __fmul_rn(dx, sin_xt);
     float ldx = 0.0f, ldy = 0.0f;
     bool use_l = false;
-    if (a.has_local) use_l = local_interp(a.loc, v, (float)oxc, (float)iy, ldx, ldy);
+    if (a.has_local) use_l = local_corr(a.loc, v, oxc, iy, a.ny, ldx, ldy);
     float sample_y = __fadd_rn((float)iy, yoff);
     if (use_l) sample_y = __fadd_rn(sample_y, ldy);
     const float fly = floorf(sample_y);

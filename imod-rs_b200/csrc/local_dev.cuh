@@ -41,4 +41,17 @@ __device__ __forceinline__ bool local_interp(const LocalDev &L, int v, float x, 
   return true;
 }
 
+// The correction at column ox (an integer column, as every caller passes) of
+// slice iy: from the per-session table when there is one.
+__device__ __forceinline__ bool local_corr(const LocalDev &L, int v, int ox, int iy, int ny, float &odx,
+                                           float &ody) {
+  if (L.table) {
+    const float2 t = __ldg(&L.table[((size_t)v * ny + iy) * L.table_nx + ox]);
+    odx = t.x;
+    ody = t.y;
+    return true;  // (0, 0) for views without patches: adding it changes nothing
+  }
+  return local_interp(L, v, (float)ox, (float)iy, odx, ody);
+}
+
 }  // namespace tg

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(128) fp_kernel(FpArgs a) {
         for (int iy = iy_lo; iy <= iy_hi; ++iy) {
           float ldx = 0.0f, ldy = 0.0f;
           bool use_l = false;
-          if (a.has_local) use_l = local_interp(a.loc, v, (float)ox, (float)iy, ldx, ldy);
+          if (a.has_local) use_l = local_corr(a.loc, v, ox, iy, a.ny, ldx, ldy);
           const float x = use_l ? __fadd_rn(xb, ldx) : xb;
           const float fx = floorf(x);
           if (!(fx >= 0.0f && fx + 1.0f < (float)a.nx)) continue;
@@ -513,6 +513,103 @@ static void launch_fast(const FpArgs &a, cudaStream_t st) {
 
 int fp_group_rows(int variant) { return variant == 1 || variant == 3 ? 16 : 8; }
 
+// ---- local alignment ----
+// The table of corrections: ViewPatches::interpolate (main.rs:172-228) at every
+// integer column of every slice of every view, computed once per session with
+// the same f32 expressions as local_interp.
+__global__ void local_table_kernel(LocalDev L, int nviews, int ny, int onx, float2 *table) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t n = (size_t)nviews * ny * onx;
+  if (i >= n) return;
+  const int ox = (int)(i % onx);
+  const size_t r = i / onx;
+  const int iy = (int)(r % ny), v = (int)(r / ny);
+  float dx = 0.0f, dy = 0.0f;
+  local_interp(L, v, (float)ox, (float)iy, dx, dy);
+  table[i] = make_float2(dx, dy);
+}
+
+void launch_local_table(const LocalDev &L, int nviews, int ny, int onx, float2 *table, cudaStream_t st) {
+  const size_t n = (size_t)nviews * ny * onx;
+  local_table_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(L, nviews, ny, onx, table);
+}
+
+// Reprojection with local alignment: one thread owns bin p of S rows of one view
+// and gathers, per depth, every (column, slice) whose corrected position lands
+// in [p-1, p+1) and whose corrected row reaches one of its rows, with the
+// reference's weights (main.rs:831-896: with local alignment every sample splits
+// over two rows, the last row takes the one-row branch).  The corrections come
+// from the session's table; the thread's S row sums live in shared memory (the
+// target row depends on the slice's correction).  Order: z, x, slice.
+template <int S>
+__global__ void __launch_bounds__(128) fp_local_kernel(FpArgs a) {
+  __shared__ float sacc[S][128];
+  const int tid = threadIdx.x;
+  const int v = blockIdx.x;
+  const int p = blockIdx.y * blockDim.x + tid;
+  const int r0 = blockIdx.z * S;
+  if (p >= a.nx) return;
+  const int nrows = min(S, a.ny - r0);
+  float *out = a.sino + ((size_t)v * a.ny + r0) * a.nx + p;
+  if (v >= a.nviews) {  // views without a tilt angle contribute nothing (main.rs:683-686)
+    for (int s = 0; s < nrows; ++s) out[(size_t)s * a.nx] = 0.0f;
+    return;
+  }
+#pragma unroll
+  for (int s = 0; s < S; ++s) sacc[s][tid] = 0.0f;
+  const float4 g = __ldg(&a.vg[v]);
+  const float4 g2 = __ldg(&a.vg2[v]);
+  const float cos_t = g.x, sin_t = g.y, zf = g.z, cos_xt = g.w, sin_xt = g2.x;
+  const float lxmax = g2.y, lymax = g2.z;  // bounds of |dx|, |dy| of this view's corrections
+  const float aeff = cos_t * cos_xt;
+  const float inv_a = fabsf(aeff) > 1e-3f ? 1.0f / aeff : 0.0f;
+  const float pf = (float)p;
+  for (int oz = 0; oz < a.onz; ++oz) {
+    const float dz = __fsub_rn((float)oz, a.cz);
+    const float t2 = __fmul_rn(__fmul_rn(dz, sin_t), zf);
+    int lo = 0, hi = a.onx - 1;
+    if (inv_a != 0.0f) {
+      const float base = a.cx + t2;
+      const float d1 = (pf - 1.0f - lxmax - base) * inv_a, d2 = (pf + 1.0f + lxmax - base) * inv_a;
+      const float dmin = fmaxf(fminf(d1, d2) + a.ocx, -1.0f), dmax = fminf(fmaxf(d1, d2) + a.ocx, (float)a.onx);
+      lo = max((int)floorf(dmin) - 1, 0);
+      hi = min((int)ceilf(dmax) + 1, a.onx - 1);
+    }
+    for (int ox = lo; ox <= hi; ++ox) {
+      const float dx = __fsub_rn((float)ox, a.ocx);
+      const float xb = __fadd_rn(__fadd_rn(__fmul_rn(__fmul_rn(dx, cos_t), cos_xt), t2), a.cx);
+      const float yoff = __fmul_rn(dx, sin_xt);
+      // slices whose corrected row can reach rows [r0, r0 + nrows)
+      const int iy_lo = max((int)floorf((float)r0 - 2.0f - yoff - lymax), 0);
+      const int iy_hi = min((int)ceilf((float)(r0 + nrows) + 1.0f - yoff + lymax), a.ny - 1);
+      for (int iy = iy_lo; iy <= iy_hi; ++iy) {
+        const float2 l = __ldg(&a.loc.table[((size_t)v * a.ny + iy) * a.loc.table_nx + ox]);
+        const float x = __fadd_rn(xb, l.x);
+        const float fx = floorf(x);
+        if (!(fx >= 0.0f && fx + 1.0f < (float)a.nx)) continue;
+        const int x0 = (int)fx;
+        if (x0 != p && x0 != p - 1) continue;
+        const float sy = __fadd_rn(__fadd_rn((float)iy, yoff), l.y);
+        const float fsy = floorf(sy);
+        if (!(fsy >= 0.0f && fsy < (float)a.ny)) continue;
+        const int s0 = (int)fsy - r0;
+        if (s0 < -1 || s0 >= nrows) continue;
+        const float frac = __fsub_rn(x, fx);
+        const float val = __ldg(a.vol + ((size_t)iy * a.onz + oz) * a.onx + ox);
+        const float c = x0 == p ? __fmul_rn(val, __fsub_rn(1.0f, frac)) : __fmul_rn(val, frac);
+        if ((int)fsy + 1 < a.ny) {  // two rows (always with local alignment, main.rs:877)
+          const float syf = __fsub_rn(sy, fsy);
+          if (s0 >= 0) sacc[s0][tid] = __fadd_rn(sacc[s0][tid], __fmul_rn(c, __fsub_rn(1.0f, syf)));
+          if (s0 + 1 < nrows) sacc[s0 + 1][tid] = __fadd_rn(sacc[s0 + 1][tid], __fmul_rn(c, syf));
+        } else if (s0 >= 0) {
+          sacc[s0][tid] = __fadd_rn(sacc[s0][tid], c);
+        }
+      }
+    }
+  }
+  for (int s = 0; s < nrows; ++s) out[(size_t)s * a.nx] = sacc[s][tid];
+}
+
 void launch_reproject(const FpArgs &a, cudaStream_t st) {
   if ((a.fast == 1 || a.fast == 2) && a.volh) {
     if (fp_half_rows(a.variant) == 32) launch_half<32>(a, st);
@@ -522,6 +619,12 @@ void launch_reproject(const FpArgs &a, cudaStream_t st) {
   if (a.fast) {
     if (fp_group_rows(a.variant) == 16) launch_fast<16>(a, st);
     else launch_fast<8>(a, st);
+    return;
+  }
+  if (a.has_local && a.loc.table) {
+    constexpr int S = 8;
+    dim3 grid(a.nviews_all, (a.nx + 127) / 128, (a.ny + S - 1) / S);
+    fp_local_kernel<S><<<grid, 128, 0, st>>>(a);
     return;
   }
   dim3 grid((a.nx + 127) / 128, a.ny, a.nviews_all);

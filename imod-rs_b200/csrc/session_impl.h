@@ -38,6 +38,7 @@ struct tg_session {  // one tilt series resident on a device
   int4 *d_lvinfo = nullptr;
   int *d_lgoff = nullptr;
   float *d_lxs = nullptr, *d_lys = nullptr, *d_lgdx = nullptr, *d_lgdy = nullptr;
+  float2 *d_ltab = nullptr;  // local corrections per (view, slice, column)
   FftPlanDev plan{};
   bool use_conv = false;
   bool uploaded = false, prepared = false;

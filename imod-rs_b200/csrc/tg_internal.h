@@ -71,6 +71,10 @@ struct LocalDev {
   const int4 *vinfo;        // (x_off, nxs, y_off, nys)
   const int *goff;          // grid offset per view
   const float *xs, *ys, *gdx, *gdy;
+  // per (view, slice, column): the interpolated (dx, dy) of local_interp, or null.
+  // Views without patches hold (0, 0); adding 0 changes no position.
+  const float2 *table;
+  int table_nx;             // columns per table row (the output width)
 };
 struct BpArgs {
   const void *pairs;
@@ -138,6 +142,8 @@ struct FpArgs {
                             // bit 3: FP32 reprojection also for half staging
 };
 void launch_reproject(const FpArgs &a, cudaStream_t st);
+// fills L.table for every (view < nviews, slice < ny, column < onx)
+void launch_local_table(const LocalDev &L, int nviews, int ny, int onx, float2 *table, cudaStream_t st);
 int fp_group_rows(int variant);
 int fp_half_rows(int variant);
 

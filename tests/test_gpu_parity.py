@@ -112,6 +112,36 @@ def test_whole_path_fp32(nx):
     assert abs(st["amean"] - rst["amean"]) <= 1e-4 * max(abs(rst["amean"]), 1e-3)
 
 
+def _local_rows(nz, nx, ny, seed, skip=()):
+    rng = np.random.default_rng(seed)
+    rows = []
+    for v in range(nz):
+        if v in skip:  # a view without patches: no correction, still the two-row split
+            continue
+        for x in np.linspace(4, nx - 5, 3):
+            for y in np.linspace(2, ny - 3, 3):
+                rows.append([v, x, y, rng.uniform(-1.5, 1.5), rng.uniform(-1.0, 1.0)])
+    return np.array(rows, np.float32)
+
+
+@pytest.mark.parametrize("ny,xt", [(16, 0.0), (13, 1.5)])
+def test_sirt_local_alignment_vs_oracle(ny, xt):
+    # local corrections from the per-session table, in the back-projector (bit-exact
+    # alone) and in the multi-row reprojector (summation order differs: tolerance)
+    nz, nx = 11, 44
+    proj = random_stack(nz, ny, nx, seed=80 + ny)
+    ang = angles(-50, 50, 10)
+    kw = dict(sirt=2, sirt_relax=0.9, no_weight=True, no_cosine_stretch=True, thickness=20,
+              local=_local_rows(nz, nx, ny, seed=ny, skip=(3,)))
+    if xt:
+        kw["xtilt"] = np.full(nz, xt, np.float32)
+    vol, _, ref, _ = both(proj, ang, **kw)
+    assert rel_l2(vol, ref) <= 1e-6
+    vol, _, ref, _ = both(smooth_stack(nz, ny, nx, seed=81), ang, sirt=2, radial=(0.35, 0.035),
+                          thickness=20, local=kw["local"])
+    assert rel_l2(vol, ref) <= TOL_FP32
+
+
 @pytest.mark.parametrize("nx,opts", [(256, dict()), (1024, dict(cosine_interp="cubic")),
                                      (384, dict()), (768, dict(fill_mode="edge", sirt=1)),
                                      (512, dict(fill_mode="edge", max_cosine_tilt=40.0)),
