@@ -534,7 +534,7 @@ void launch_local_table(const LocalDev &L, int nviews, int ny, int onx, float2 *
   local_table_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(L, nviews, ny, onx, table);
 }
 
-// Reprojection with local alignment: one thread owns bin p of S rows of one view
+// Reprojection with local alignment: one thread owns bin p of S (16) rows of one view
 // and gathers, per depth, every (column, slice) whose corrected position lands
 // in [p-1, p+1) and whose corrected row reaches one of its rows, with the
 // reference's weights (main.rs:831-896: with local alignment every sample splits
@@ -622,7 +622,7 @@ void launch_reproject(const FpArgs &a, cudaStream_t st) {
     return;
   }
   if (a.has_local && a.loc.table) {
-    constexpr int S = 8;
+    constexpr int S = 16;
     dim3 grid(a.nviews_all, (a.nx + 127) / 128, (a.ny + S - 1) / S);
     fp_local_kernel<S><<<grid, 128, 0, st>>>(a);
     return;
