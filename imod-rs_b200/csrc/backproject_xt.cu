@@ -105,7 +105,7 @@ __device__ __forceinline__ XtWindow xt_window(const BpArgs &a, float4 g, float s
 }  // namespace
 
 template <int STORE, int S, int K>
-__global__ void __launch_bounds__(XT_TX * XT_NW) bp_xtilt_kernel(BpArgs a) {
+__global__ void __launch_bounds__(XT_TX * XT_NW, 5) bp_xtilt_kernel(BpArgs a) {
   constexpr int TZ = XT_NW * K, RMAX = S + 8;
   constexpr int EB = STORE == TG_STORE_FP32 ? 8 : 4;
   __shared__ __align__(16) unsigned char stage[2][RMAX * XT_WMAX * EB];
