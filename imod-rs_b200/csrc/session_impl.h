@@ -15,7 +15,7 @@ struct tg_session {  // one tilt series resident on a device
   bool has_local = false, fast = true, zf_any = false;
   bool xt_fast = false;  // not fast: x-tilt back-projection with staged rows instead of the general kernel
   int fp_fast = 0;  // reprojector: 0 general, 1 fast (no x-tilt), 2 fast with x-tilt
-  bool xt_common = false;  // every view has the same x-tilt (sheared copy for the reprojector)
+  bool xt_common = false;  // every view has the same x-tilt (blended copy for the reprojector)
   float sin_xt_common = 0.0f;
   int fp_variant = 2;  // reprojector variant bits (FpArgs::variant); TG_FP_VARIANT overrides
   float *d_volg = nullptr;  // interleaved copy of the volume for the reprojector
