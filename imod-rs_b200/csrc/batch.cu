@@ -151,6 +151,7 @@ int tg_batch_reconstruct(tg_batch *b) {
   for (tg_session *s : b->sess) max_it = std::max(max_it, sirt_iters(s));
   // round r: the r-th SIRT update of every series that still iterates
   for (int r = 1; r <= max_it; ++r) {
+    NvtxRange nv("tg.batch.sirt_round");
     std::vector<tg_session *> act;
     for (tg_session *s : b->sess)
       if (sirt_iters(s) >= r) {

@@ -267,6 +267,7 @@ void admit_loop(tg_server *sv) {
       continue;
     }
     const auto t_adm = std::chrono::steady_clock::now();
+    NvtxRange nv("tg.server.admit");
     tg_session *s = nullptr;
     int rc = session_create_ex(&j->g, &j->o, sv->pool, false, fail_alloc, &s);
     if (rc == TG_ERR_OOM && !fail_alloc && j->oom_retries < kMaxOomRetries) {
@@ -349,6 +350,7 @@ bool run_round(tg_server *sv) {
   }
   if (ready.empty()) return false;
   const auto t_host = std::chrono::steady_clock::now();
+  NvtxRange nv("tg.server.round");
   cudaEvent_t r0 = take_timing_event(sv);
   if (r0) cudaEventRecord(r0, sv->cs);
   std::vector<tg_session *> ss;

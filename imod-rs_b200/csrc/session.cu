@@ -745,14 +745,21 @@ int tg_reconstruct(tg_session *s) {
   const int iters = sirt_iters(s);
   s->timed = false;
   TG_CUDA(cudaEventRecord(s->ev[0], s->st));
-  if ((rc = stage_front(s, &launches)) != TG_OK) return rc;
+  {
+    NvtxRange r("tg.filter");
+    if ((rc = stage_front(s, &launches)) != TG_OK) return rc;
+  }
   TG_CUDA(cudaEventRecord(s->ev[1], s->st));
   const int mode0 = first_mode(s);
-  if ((rc = launch_bp(s, mode0, &ntiles)) != TG_OK) return rc;
+  {
+    NvtxRange r("tg.backproject");
+    if ((rc = launch_bp(s, mode0, &ntiles)) != TG_OK) return rc;
+  }
   launches++;
   TG_CUDA(cudaGetLastError());
   TG_CUDA(cudaEventRecord(s->ev[2], s->st));
   if (iters > 0) {
+    NvtxRange r("tg.sirt");
     auto one_iter = [&]() -> int {
       launch_reproject(fp_args(s), s->st);
       launch_filter(filter_args(s, true), s->st);
@@ -778,7 +785,10 @@ int tg_reconstruct(tg_session *s) {
     launches += 3 * iters;
   }
   TG_CUDA(cudaEventRecord(s->ev[3], s->st));
-  if ((rc = stage_finish(s, mode0, ntiles, &launches)) != TG_OK) return rc;
+  {
+    NvtxRange r("tg.finish");
+    if ((rc = stage_finish(s, mode0, ntiles, &launches)) != TG_OK) return rc;
+  }
   TG_CUDA(cudaEventRecord(s->ev[4], s->st));
   s->info = tg_run_info{};
   s->info.passes = 1 + iters;

@@ -7,6 +7,8 @@
 
 #include "../../include/tiltgpu.h"
 
+#include <nvtx3/nvToolsExt.h>  // header-only NVTX v3: no-ops unless a profiler is attached
+
 namespace tg {
 
 // Staged-projection formats written by the filter stage and read by the
@@ -162,6 +164,13 @@ int synth_projections(const tg_phantom_spec *spec, const float *angles, float *d
 
 // ---- errors ----
 void set_error(const std::string &msg);
+// NVTX range over a host scope (the kernels launched inside it, for ncu --nvtx filters)
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 int cuda_fail(cudaError_t e, const char *what);
 #define TG_STR2(x) #x
 #define TG_STR(x) TG_STR2(x)
