@@ -637,6 +637,9 @@ int tg_server_inject(tg_server *sv, int32_t fault, int32_t count) {
   return TG_OK;
 }
 
+int tg_submit(tg_server *sv, const tg_job *job, uint64_t *id) { return tg_server_submit(sv, job, id); }
+int tg_poll(tg_server *sv, uint64_t id, tg_job_result *out) { return tg_server_poll(sv, id, out); }
+
 int tg_server_destroy(tg_server *sv) {
   if (!sv) return TG_ERR_INVALID_ARG;
   {

@@ -150,6 +150,8 @@ EXPORTS = {
     "tg_server_get_info": (C.c_int, [_P, C.POINTER(ServerInfo)]),
     "tg_server_inject": (C.c_int, [_P, _i32, _i32]),
     "tg_server_destroy": (C.c_int, [_P]),
+    "tg_submit": (C.c_int, [_P, C.POINTER(Job), C.POINTER(C.c_uint64)]),
+    "tg_poll": (C.c_int, [_P, C.c_uint64, C.POINTER(JobResult)]),
 }
 # library-internal helpers exported for tests and the benchmark (not in the header)
 EXTRA = {

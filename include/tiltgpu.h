@@ -229,6 +229,9 @@ int tg_server_get_info(tg_server *sv, tg_server_info *out);
 int tg_server_inject(tg_server *sv, int32_t fault, int32_t count);
 /* Drops queued jobs (TG_ERR_CANCELLED), lets running jobs finish, stops the device thread. */
 int tg_server_destroy(tg_server *sv);
+/* Short names of tg_server_submit / tg_server_poll. */
+int tg_submit(tg_server *sv, const tg_job *job, uint64_t *id);
+int tg_poll(tg_server *sv, uint64_t id, tg_job_result *out);
 
 /* ---- The reference's GPU seam, same arguments and meaning ----
  * GpuSession::new(projections, tilt_cos_sin, in_nx, in_ny, n_projs, out_nx, out_nz)
