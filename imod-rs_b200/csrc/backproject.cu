@@ -30,6 +30,7 @@
 #include <type_traits>
 
 #include "tg_internal.h"
+#include "f32x2.cuh"
 #include "local_dev.cuh"
 
 namespace tg {
@@ -105,28 +106,6 @@ __device__ __forceinline__ void add2_f32_bf16(float &acc0, float &acc1, uint32_t
       : "r"(h2));
 }
 
-// Packed FP32x2 arithmetic (PTX 8.6, sm_100+): two IEEE round-to-nearest f32
-// operations per instruction, each lane identical to the scalar operation.
-__device__ __forceinline__ uint64_t pk2(float lo, float hi) {
-  uint64_t d;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
-  return d;
-}
-__device__ __forceinline__ float2 up2(uint64_t v) {
-  float2 r;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
-  return r;
-}
-__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
-  uint64_t d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
-  uint64_t d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
 
 // Shared loads at a 32-bit shared address plus a compile-time byte offset,
 // ordered after the mbarrier waits (all are volatile asm).
@@ -253,8 +232,8 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
   // ---- per-view windows of this tile (x is monotone in dx and dz: corners bound it)
   for (int v = tid; v < a.nviews; v += C::NTHR) {
     float4 g = __ldg(&a.vg[v]);
-    float t1l = __fmul_rn(__fsub_rn((float)oxlo, a.ocx), g.x);
-    float t1h = __fmul_rn(__fsub_rn((float)oxhi, a.ocx), g.x);
+    float t1l = __fmul_rn(__fmul_rn(__fsub_rn((float)oxlo, a.ocx), g.x), g.w);
+    float t1h = __fmul_rn(__fmul_rn(__fsub_rn((float)oxhi, a.ocx), g.x), g.w);
     float dzl = __fsub_rn((float)ozlo, a.cz), dzh = __fsub_rn((float)ozhi, a.cz);
     float x0 = ref_x<ZF>(t1l, dzl, g.y, g.z, a.cx), x1 = ref_x<ZF>(t1l, dzh, g.y, g.z, a.cx);
     float x2 = ref_x<ZF>(t1h, dzl, g.y, g.z, a.cx), x3 = ref_x<ZF>(t1h, dzh, g.y, g.z, a.cx);
@@ -350,7 +329,8 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
       if (vi < nv) {
         const int v = v0 + vi;
         const float4 g = __ldg(&a.vg[v]);
-        const float t1 = __fmul_rn(dx, g.x);  // (dx*cos_t)*cos_xt, cos_xt == 1 exactly here
+        // (dx*cos_t)*cos_xt; cos_xt is 1 exactly without x-tilt (the product is then dx*cos_t)
+        const float t1 = __fmul_rn(__fmul_rn(dx, g.x), g.w);
         // half staging (a tolerance path): one FMA per position, x within an ulp of the
         // reference's; linear interpolation is continuous, so a floor moved by it
         // changes the sample by at most the rounding of x

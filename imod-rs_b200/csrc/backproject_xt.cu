@@ -296,6 +296,87 @@ __global__ void __launch_bounds__(XT_TX * XT_NW, 5) bp_xtilt_kernel(BpArgs a) {
   }
 }
 
+// Row-sum form of the x-tilt back-projection (all views share one x-tilt).
+// With a common x-tilt the row pair and fraction of voxel (ox, iy) are the same
+// in every view, so the reference's sum over views of v0*(1-f) + v1*f
+// (main.rs:802-817, 1045-1063) is B[sy0]*(1-f) + B[sy0+1]*f, B[r] the view sum
+// of the row-r samples: the fast kernel's no-x-tilt pass with x =
+// ((dx*cos)*cos_xt + (dz*sin)*zf) + cx, which already carries the 1/N.  The row
+// choice below is the reference's f32 expression; only the order of the f32
+// sums differs.  Block (t, iy): depths [onz*t/XB_TILES, onz*(t+1)/XB_TILES) of
+// slice iy, a warp on 32 consecutive columns of one depth row (coalesced);
+// slices run in order so the rows that neighbouring slices share stay in L2.
+template <int MODE>
+__global__ void __launch_bounds__(256) xt_blend_kernel(BpArgs a, const float *__restrict__ rows, float sin_xt) {
+  const int t = blockIdx.x, iy = blockIdx.y;
+  const int oz0 = (int)((long long)a.onz * t / XB_TILES), oz1 = (int)((long long)a.onz * (t + 1) / XB_TILES);
+  const size_t sl = (size_t)a.onz * a.onx;
+  float mn = 3.40282347e+38f, mx = -3.40282347e+38f;
+  double sum = 0.0;
+  const float fiy = (float)iy;
+  for (int ox = threadIdx.x; ox < a.onx; ox += blockDim.x) {
+    const float yoff = __fmul_rn(__fsub_rn((float)ox, a.ocx), sin_xt);
+    const float sy = __fadd_rn(fiy, yoff);
+    const float fl = floorf(sy);
+    const int sy0 = (int)fl;
+    const float fr = __fsub_rn(sy, fl);
+    const bool two = sy0 >= 0 && sy0 + 1 < a.ny && fabsf(yoff) > 1e-6f;
+    const bool one = !two && sy0 >= 0 && sy0 < a.ny;
+    const float w0 = __fsub_rn(1.0f, fr);
+    const float *b0 = rows + ((two || one) ? (size_t)sy0 * sl : 0) + ox;
+    float *out = a.vol + (size_t)iy * sl + ox;
+#pragma unroll 4
+    for (int oz = oz0; oz < oz1; ++oz) {
+      const size_t o = (size_t)oz * a.onx;
+      float v = 0.0f;
+      if (two) v = __fadd_rn(__fmul_rn(__ldg(b0 + o), w0), __fmul_rn(__ldg(b0 + sl + o), fr));
+      else if (one) v = __ldg(b0 + o);
+      if (MODE == 0) {
+        const float y = __fadd_rn(__fmul_rn(__fmul_rn(v, a.dw), a.os), a.oa);
+        out[o] = y;
+        mn = fminf(mn, y);
+        mx = fmaxf(mx, y);
+        sum += (double)y;
+      } else if (MODE == 1) {
+        out[o] = v;
+      } else {
+        out[o] = __fadd_rn(out[o], __fmul_rn(a.relax, v));
+      }
+    }
+  }
+  if (MODE == 0) {
+    __shared__ float rmn[8], rmx[8];
+    __shared__ double rs[8];
+    for (int o = 16; o > 0; o >>= 1) {
+      mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+      mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { rmn[w] = mn; rmx[w] = mx; rs[w] = sum; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      StatPartial p;
+      p.mn = rmn[0];
+      p.mx = rmx[0];
+      p.sum = rs[0];
+      for (int k = 1; k < 8; ++k) { p.mn = fminf(p.mn, rmn[k]); p.mx = fmaxf(p.mx, rmx[k]); p.sum += rs[k]; }
+      a.partial[(size_t)iy * XB_TILES + t] = p;
+    }
+  }
+}
+
+int launch_xt_blend(const BpArgs &a, const float *rows, float sin_xt, cudaStream_t st, int *ntiles) {
+  if (ntiles) *ntiles = XB_TILES;
+  if (a.ny <= 0 || a.onx <= 0 || a.onz <= 0) return TG_OK;
+  if (a.ny > 65535) { set_error("more than 65535 rows"); return TG_ERR_UNSUPPORTED; }
+  const dim3 grid(XB_TILES, a.ny);
+  if (a.mode == 0) xt_blend_kernel<0><<<grid, 256, 0, st>>>(a, rows, sin_xt);
+  else if (a.mode == 1) xt_blend_kernel<1><<<grid, 256, 0, st>>>(a, rows, sin_xt);
+  else xt_blend_kernel<2><<<grid, 256, 0, st>>>(a, rows, sin_xt);
+  return TG_OK;
+}
+
 bool bp_xtilt_supported(int onx, float max_abs_sin_xt, float max_x_extent_per_tile) {
   (void)onx;
   // rows a 32-column tile can reach: S + 2 + (nhi - nlo) <= S + 8, and the element window <= 72

@@ -29,7 +29,7 @@ int batch_bp(tg_batch *b, const std::vector<tg_session *> &ss, const std::vector
     else {
       int rc = launch_bp(ss[i], modes[i], &ntiles[i]);
       if (rc != TG_OK) return rc;
-      ++*launches;
+      *launches += bp_launch_count(ss[i]);
     }
   }
   for (auto &kv : groups) {
@@ -155,9 +155,9 @@ int tg_batch_reconstruct(tg_batch *b) {
     std::vector<tg_session *> act;
     for (tg_session *s : b->sess)
       if (sirt_iters(s) >= r) {
-        launch_reproject(fp_args(s), s->st);
+        launches += launch_reproject(fp_args(s), s->st);
         launch_filter(filter_args(s, true), s->st);
-        launches += 2;
+        launches += 1;
         act.push_back(s);
       }
     std::vector<int> m2(act.size(), 2);

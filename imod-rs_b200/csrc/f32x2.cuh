@@ -1,0 +1,30 @@
+// f32x2.cuh -- packed FP32x2 arithmetic (PTX 8.6, sm_100+): two IEEE
+// round-to-nearest f32 operations per instruction, each lane identical to the
+// scalar operation (so packed sums and products keep bit-exact results).
+#pragma once
+#include <cstdint>
+
+namespace tg {
+
+__device__ __forceinline__ uint64_t pk2(float lo, float hi) {
+  uint64_t d;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+  return d;
+}
+__device__ __forceinline__ float2 up2(uint64_t v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+}  // namespace tg

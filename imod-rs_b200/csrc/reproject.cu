@@ -11,6 +11,7 @@
 #include <cuda_fp16.h>
 
 #include "tg_internal.h"
+#include "f32x2.cuh"
 #include "local_dev.cuh"
 
 namespace tg {
@@ -146,24 +147,29 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
   float acc[S];
 #pragma unroll
   for (int s = 0; s < S; ++s) acc[s] = 0.0f;
-  auto X = [&](int ox, float t2) {  // ((dx*cos)*cos_xt + t2) + cx, exactly as main.rs:842
-    const float dx = __fsub_rn((float)ox, a.ocx);
+  // ((dx*cos)*cos_xt + t2) + cx, exactly as main.rs:842; fo is the column as a float
+  // (carried along with the integer column: integers are exact in f32)
+  auto X = [&](float fo, float t2) {
+    const float dx = __fsub_rn(fo, a.ocx);
     const float t1 = XT ? __fmul_rn(__fmul_rn(dx, cos_t), cos_xt) : __fmul_rn(dx, cos_t);
     return __fadd_rn(__fadd_rn(t1, t2), a.cx);
   };
   // XT: row r0+s is the last row of the series (one-row branch) when s == last_s
   const int last_s = a.ny - 1 - r0;
-  for (int oz = 0; oz < a.onz; ++oz) {
-    const float dz = __fsub_rn((float)oz, a.cz);
+  float foz = 0.0f;
+  for (int oz = 0; oz < a.onz; ++oz, foz += 1.0f) {
+    const float dz = __fsub_rn(foz, a.cz);
     const float t2 = __fmul_rn(__fmul_rn(dz, sin_t), zf);
     // first column whose position is >= p-1
     int lo = (int)floorf((lo_t - a.cx - t2) * inv_a + a.ocx) - 1;
     lo = min(max(lo, 0), a.onx);
-    while (lo > 0 && X(lo - 1, t2) >= lo_t) --lo;
-    while (lo < a.onx && X(lo, t2) < lo_t) ++lo;
+    float flo = (float)lo;
+    while (lo > 0 && X(flo - 1.0f, t2) >= lo_t) { --lo; flo -= 1.0f; }
+    while (lo < a.onx && X(flo, t2) < lo_t) { ++lo; flo += 1.0f; }
     const float *vz = a.vol + (size_t)oz * a.onx;
-    for (int ox = lo; ox < a.onx; ++ox) {
-      const float x = X(ox, t2);
+    float fo = flo;
+    for (int ox = lo; ox < a.onx; ++ox, fo += 1.0f) {
+      const float x = X(fo, t2);
       if (!(x < hi_t)) break;
       const float tt = __fadd_rd(x, FMAGIC);
       const int x0 = (int)(__float_as_uint(tt) - FMAGIC_BITS);
@@ -175,13 +181,17 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
         // x-tilt each holds the row's blend of its two source slices (blend_interleave_kernel)
         const float4 *q = reinterpret_cast<const float4 *>(a.volg) +
                           (((size_t)blockIdx.z * a.onz + oz) * a.onx + ox) * (S / 4);
+        // products on the f32x2 pipe; the sums stay scalar so that no product is
+        // contracted into them (each stays RN(acc + RN(v*w)), the reference's operations)
+        const uint64_t w2 = pk2(w, w);
 #pragma unroll
         for (int k = 0; k < S / 4; ++k) {
           const float4 q4 = __ldg(q + k);
-          acc[4 * k + 0] = __fadd_rn(acc[4 * k + 0], __fmul_rn(q4.x, w));
-          acc[4 * k + 1] = __fadd_rn(acc[4 * k + 1], __fmul_rn(q4.y, w));
-          acc[4 * k + 2] = __fadd_rn(acc[4 * k + 2], __fmul_rn(q4.z, w));
-          acc[4 * k + 3] = __fadd_rn(acc[4 * k + 3], __fmul_rn(q4.w, w));
+          const float2 pa = up2(mul2(pk2(q4.x, q4.y), w2)), pb = up2(mul2(pk2(q4.z, q4.w), w2));
+          acc[4 * k + 0] = __fadd_rn(acc[4 * k + 0], pa.x);
+          acc[4 * k + 1] = __fadd_rn(acc[4 * k + 1], pa.y);
+          acc[4 * k + 2] = __fadd_rn(acc[4 * k + 2], pb.x);
+          acc[4 * k + 3] = __fadd_rn(acc[4 * k + 3], pb.y);
         }
       } else if (!XT) {
         const float *vrow = vz + (size_t)r0 * sstride + ox;
@@ -189,7 +199,7 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
         for (int s = 0; s < S; ++s)
           if (s < nrows) acc[s] = __fadd_rn(acc[s], __fmul_rn(__ldg(vrow + (size_t)s * sstride), w));
       } else {
-        const float yoff = __fmul_rn(__fsub_rn((float)ox, a.ocx), sin_xt);
+        const float yoff = __fmul_rn(__fsub_rn(fo, a.ocx), sin_xt);
         const float fn = floorf(yoff);
         const int iy0 = r0 - 1 - (int)fn;  // slice of i = 0
         const float *vcol = vz + ox;
@@ -356,19 +366,22 @@ __global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
   // ((dx*cos)*cos_xt + t2) + cx, and non-decreasing in ox, which the search needs)
   const float c = XT ? cos_t * cos_xt : cos_t;
   float c0 = 0.0f;
-  auto X = [&](int ox, float) { return fmaf((float)ox, c, c0); };
+  auto X = [&](float fo) { return fmaf(fo, c, c0); };  // fo: the column as a float
   const uint4 *vg = reinterpret_cast<const uint4 *>(a.volh) + (size_t)blockIdx.z * a.onz * a.onx * (S / 8);
-  for (int oz = 0; oz < a.onz; ++oz) {
-    const float dz = __fsub_rn((float)oz, a.cz);
+  float foz = 0.0f;
+  for (int oz = 0; oz < a.onz; ++oz, foz += 1.0f) {
+    const float dz = __fsub_rn(foz, a.cz);
     const float t2 = __fmul_rn(__fmul_rn(dz, sin_t), zf);
     c0 = fmaf(-a.ocx, c, t2 + a.cx);
     int lo = (int)floorf((lo_t - a.cx - t2) * inv_a + a.ocx) - 1;
     lo = min(max(lo, 0), a.onx);
-    while (lo > 0 && X(lo - 1, t2) >= lo_t) --lo;
-    while (lo < a.onx && X(lo, t2) < lo_t) ++lo;
+    float flo = (float)lo;
+    while (lo > 0 && X(flo - 1.0f) >= lo_t) { --lo; flo -= 1.0f; }
+    while (lo < a.onx && X(flo) < lo_t) { ++lo; flo += 1.0f; }
     const uint4 *vz = vg + (size_t)oz * a.onx * (S / 8);
-    for (int ox = lo; ox < a.onx; ++ox) {
-      const float x = X(ox, t2);
+    float fo = flo;
+    for (int ox = lo; ox < a.onx; ++ox, fo += 1.0f) {
+      const float x = X(fo);
       if (!(x < hi_t)) break;
       const float tt = __fadd_rd(x, FMAGIC);
       const int x0 = (int)(__float_as_uint(tt) - FMAGIC_BITS);
@@ -475,7 +488,7 @@ __global__ void blend_interleave_half_kernel(const float *__restrict__ vol, __ha
 }
 
 template <int S>
-static void launch_half(const FpArgs &a, cudaStream_t st) {
+static int launch_half(const FpArgs &a, cudaStream_t st) {
   const size_t nvol = (size_t)a.ny * a.onz * a.onx;
   cudaMemsetAsync(a.maxbits, 0, sizeof(unsigned), st);
   absmax_kernel<<<8 * 148, 256, 0, st>>>(a.vol, nvol, a.maxbits);
@@ -490,25 +503,29 @@ static void launch_half(const FpArgs &a, cudaStream_t st) {
     interleave_half_kernel<S><<<nb, 256, 0, st>>>(a.vol, (__half *)a.volh, a.ny, a.onz, a.onx, n, a.maxbits);
     fp_half_kernel<S, false><<<grid, 128, 0, st>>>(a);
   }
+  return 3;
 }
 
 template <int S>
-static void launch_fast(const FpArgs &a, cudaStream_t st) {
+static int launch_fast(const FpArgs &a, cudaStream_t st) {
   dim3 grid(a.nviews_all, (a.nx + 127) / 128, (a.ny + S - 1) / S);
   if (a.fast == 2 && a.volg) {
     const size_t n = (size_t)((a.ny + S - 1) / S) * a.onz * a.onx;
     blend_interleave_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.vol, a.volg, a.ny, a.onz, a.onx,
                                                                           a.ocx, a.sin_xt_common, n);
     fp_fast_kernel<S, true, true><<<grid, 128, 0, st>>>(a);
+    return 2;
   } else if (a.fast == 2) {
     fp_fast_kernel<S, true, false><<<grid, 128, 0, st>>>(a);
+    return 1;
   } else if (a.volg) {
     const size_t n = (size_t)((a.ny + S - 1) / S) * a.onz * a.onx;
     interleave_kernel<S><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a.vol, a.volg, a.ny, a.onz, a.onx, n);
     fp_fast_kernel<S, false, true><<<grid, 128, 0, st>>>(a);
-  } else {
-    fp_fast_kernel<S, false, false><<<grid, 128, 0, st>>>(a);
+    return 2;
   }
+  fp_fast_kernel<S, false, false><<<grid, 128, 0, st>>>(a);
+  return 1;
 }
 
 int fp_group_rows(int variant) { return variant == 1 || variant == 3 ? 16 : 8; }
@@ -610,25 +627,19 @@ __global__ void __launch_bounds__(128) fp_local_kernel(FpArgs a) {
   for (int s = 0; s < nrows; ++s) out[(size_t)s * a.nx] = sacc[s][tid];
 }
 
-void launch_reproject(const FpArgs &a, cudaStream_t st) {
-  if ((a.fast == 1 || a.fast == 2) && a.volh) {
-    if (fp_half_rows(a.variant) == 32) launch_half<32>(a, st);
-    else launch_half<16>(a, st);
-    return;
-  }
-  if (a.fast) {
-    if (fp_group_rows(a.variant) == 16) launch_fast<16>(a, st);
-    else launch_fast<8>(a, st);
-    return;
-  }
+int launch_reproject(const FpArgs &a, cudaStream_t st) {
+  if ((a.fast == 1 || a.fast == 2) && a.volh)
+    return fp_half_rows(a.variant) == 32 ? launch_half<32>(a, st) : launch_half<16>(a, st);
+  if (a.fast) return fp_group_rows(a.variant) == 16 ? launch_fast<16>(a, st) : launch_fast<8>(a, st);
   if (a.has_local && a.loc.table) {
     constexpr int S = 16;
     dim3 grid(a.nviews_all, (a.nx + 127) / 128, (a.ny + S - 1) / S);
     fp_local_kernel<S><<<grid, 128, 0, st>>>(a);
-    return;
+    return 1;
   }
   dim3 grid((a.nx + 127) / 128, a.ny, a.nviews_all);
   fp_kernel<<<grid, 128, 0, st>>>(a);
+  return 1;
 }
 
 }  // namespace tg

@@ -298,7 +298,7 @@ void admit_loop(tg_server *sv) {
     j->s = s;
     s->st = sv->cs;
     s->variant = tune_lookup(s);
-    if (s->variant < 0) s->variant = s->fast ? 8 : 0;  // S8K4TX32NT256V4N3: best or near on the measured shapes
+    if (s->variant < 0) s->variant = s->fast || s->xt_split ? 8 : 0;  // S8K4TX32NT256V4N3: best or near on the measured shapes
     j->ev_up = take_event(sv);
     j->ev_fin = take_event(sv);
     j->ev_dl = take_event(sv);

@@ -145,7 +145,7 @@ static void free_session(tg_session *s) {
   void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_volh, s->d_maxbits, s->d_mpart, s->d_pairs,
                   s->d_part, s->d_slice_stats, s->d_stats3, s->d_vg, s->d_vg2, s->d_weights,
                   s->d_conv, s->d_stretch, s->d_tw, s->d_err, s->d_lvinfo, s->d_lgoff, s->d_lxs,
-                  s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab};
+                  s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab, s->d_xtb};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : s->ev)
@@ -159,7 +159,7 @@ void free_session_async(tg_session *s, cudaStream_t after) {
   void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_volh, s->d_maxbits, s->d_mpart, s->d_pairs,
                   s->d_part, s->d_slice_stats, s->d_stats3, s->d_vg, s->d_vg2, s->d_weights,
                   s->d_conv, s->d_stretch, s->d_tw, s->d_err, s->d_lvinfo, s->d_lgoff, s->d_lxs,
-                  s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab};
+                  s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab, s->d_xtb};
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, after);
   for (auto &e : s->ev)
@@ -304,6 +304,13 @@ FilterArgs filter_args(tg_session *s, bool residual) {
 int launch_bp(tg_session *s, int mode, int *ntiles) {
   BpArgs a = bp_args(s, mode);
   if (s->fast) return launch_bp_fast(a, s->store, s->zf_any, s->variant < 0 ? 0 : s->variant, s->st, ntiles);
+  if (s->xt_split) {  // per-row view sums, then the two-row blend of every voxel
+    BpArgs r = bp_args(s, 1);
+    r.vol = s->xtb;
+    int rc = launch_bp_fast(r, s->store, s->zf_any, s->variant < 0 ? 0 : s->variant, s->st, nullptr);
+    if (rc != TG_OK) return rc;
+    return launch_xt_blend(a, s->xtb, s->sin_xt_common, s->st, ntiles);
+  }
   if (s->xt_fast) return launch_bp_xtilt(a, s->store, s->st, ntiles);
   return launch_bp_general(a, s->store, s->st, ntiles);
 }
@@ -311,7 +318,7 @@ int launch_bp(tg_session *s, int mode, int *ntiles) {
 // Times each fast tile variant once on this series and keeps the fastest
 // (process-wide cache keyed by the series shape).
 int autotune(tg_session *s) {
-  if (!s->fast) { s->variant = 0; return TG_OK; }
+  if (!s->fast && !s->xt_split) { s->variant = 0; return TG_OK; }
   if (const char *env = getenv("TG_BP_VARIANT")) {  // fixed tile shape (profiling, tuning)
     int v = atoi(env);
     if (v >= 0 && v < bp_fast_variants()) { s->variant = v; return TG_OK; }
@@ -329,6 +336,7 @@ int autotune(tg_session *s) {
   TG_CUDA(cudaEventCreate(&e1));
   for (int v = 0; v < bp_fast_variants(); ++v) {
     BpArgs a = bp_args(s, 1);
+    if (s->xt_split) a.vol = s->xtb;
     int nt = 0;
     // warm + timed launch (mode 1 writes the volume, which is rewritten afterwards)
     if (launch_bp_fast(a, s->store, s->zf_any, v, s->st, &nt) != TG_OK) continue;
@@ -350,7 +358,7 @@ int autotune(tg_session *s) {
 }
 
 int tune_lookup(tg_session *s) {
-  if (!s->fast) return 0;
+  if (!s->fast && !s->xt_split) return 0;
   if (const char *env = getenv("TG_BP_VARIANT")) {
     int v = atoi(env);
     if (v >= 0 && v < bp_fast_variants()) return v;
@@ -553,7 +561,10 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
     if (s->xt_common) s->sin_xt_common = hv[0].sin_xt;
   }
   if (s->zf_any && zsmax > 2.0f) s->fast = false;
-  if (!s->fast && !s->has_local && zsmax <= 2.0f && !getenv("TG_BP_GENERAL")) {
+  // one x-tilt for every view: the fast kernel's per-row sums, blended per voxel
+  s->xt_split = !s->fast && !s->has_local && xt_any && s->xt_common && !opt->exact_xtilt &&
+                zsmax <= 2.0f && fabsf(zsmax) == zsmax && !getenv("TG_BP_GENERAL");
+  if (!s->fast && !s->xt_split && !s->has_local && zsmax <= 2.0f && !getenv("TG_BP_GENERAL")) {
     float msx = 0.0f, mext = 0.0f;
     bool ok = true;
     for (int i = 0; i < s->nviews; ++i) {
@@ -563,7 +574,7 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
     }
     s->xt_fast = ok && bp_xtilt_supported(s->onx, msx, mext);
   }
-  s->fmt = s->fast ? FMT_ROWPAIR : FMT_SINGLE;
+  s->fmt = s->fast || s->xt_split ? FMT_ROWPAIR : FMT_SINGLE;
 
   // cosine stretch factors (main.rs:446-460); the reference indexes
   // tilt_angles[p] for every section p < nz and panics if the file is short.
@@ -654,10 +665,19 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
     const int G = fp_group_rows(s->fp_variant);
     const size_t ng = (size_t)((s->ny + G - 1) / G) * G * s->onz * s->onx;
     if ((rc = dalloc(s, &s->d_volg, ng * 4))) return fail(rc);
+    s->volg_elems = ng;
   } else if (!opt->gpu_compat && opt->sirt_iters > 0 && s->fp_fast == 1 && (s->fp_variant & 2)) {
     const int G = fp_group_rows(s->fp_variant);
     const size_t ng = (size_t)((s->ny + G - 1) / G) * G * s->onz * s->onx;
     if ((rc = dalloc(s, &s->d_volg, ng * 4))) return fail(rc);
+    s->volg_elems = ng;
+  }
+  if (s->xt_split) {
+    // the row sums may live in the reprojector's FP32 copy: it is rebuilt from the
+    // volume before every reprojection and is dead while the back-projection runs
+    if (s->volg_elems >= nvol) s->xtb = s->d_volg;
+    else if ((rc = dalloc(s, &s->d_xtb, nvol * 4))) return fail(rc);
+    else s->xtb = s->d_xtb;
   }
   if (s->has_local && (rc = upload_local(s, g->local, g->local ? g->n_local : 0, vg2))) return fail(rc);
   // corrections per (view, slice, column): 8 bytes each, filled below
@@ -755,13 +775,13 @@ int tg_reconstruct(tg_session *s) {
     NvtxRange r("tg.backproject");
     if ((rc = launch_bp(s, mode0, &ntiles)) != TG_OK) return rc;
   }
-  launches++;
+  launches += bp_launch_count(s);
   TG_CUDA(cudaGetLastError());
   TG_CUDA(cudaEventRecord(s->ev[2], s->st));
   if (iters > 0) {
     NvtxRange r("tg.sirt");
     auto one_iter = [&]() -> int {
-      launch_reproject(fp_args(s), s->st);
+      s->iter_launches = launch_reproject(fp_args(s), s->st) + 1 + bp_launch_count(s);
       launch_filter(filter_args(s, true), s->st);
       return launch_bp(s, 2, nullptr);
     };
@@ -782,7 +802,7 @@ int tg_reconstruct(tg_session *s) {
       for (int it = 0; it < iters; ++it)
         if ((rc = one_iter()) != TG_OK) return rc;
     }
-    launches += 3 * iters;
+    launches += s->iter_launches * iters;  // counted when the iteration was issued or captured
   }
   TG_CUDA(cudaEventRecord(s->ev[3], s->st));
   {
@@ -897,7 +917,8 @@ int tg_session_destroy(tg_session *s) {
 int tg_session_kernel_info(tg_session *s, int32_t *fast, int32_t *variant, int32_t *fmt,
                            int32_t *padL, int32_t *PW) {
   if (!s) return TG_ERR_INVALID_ARG;
-  if (fast) *fast = s->fast ? 1 : s->xt_fast ? 2 : 0;  // 2: staged x-tilt kernel, 0: general kernel
+  // 2: staged x-tilt kernel, 3: fast kernel's row sums + blend, 0: general kernel
+  if (fast) *fast = s->fast ? 1 : s->xt_split ? 3 : s->xt_fast ? 2 : 0;
   if (variant) *variant = s->variant;
   if (fmt) *fmt = s->fmt;
   if (padL) *padL = s->padL;

@@ -14,11 +14,17 @@ struct tg_session {  // one tilt series resident on a device
   tg_options o{};
   bool has_local = false, fast = true, zf_any = false;
   bool xt_fast = false;  // not fast: x-tilt back-projection with staged rows instead of the general kernel
+  // x-tilt shared by all views: the fast kernel sums every projection row over the
+  // views into xtb, then launch_xt_blend blends two rows per voxel into the volume
+  bool xt_split = false;
+  float *xtb = nullptr;    // row sums (d_xtb, or the reprojector's FP32 copy, which is dead then)
+  float *d_xtb = nullptr;
   int fp_fast = 0;  // reprojector: 0 general, 1 fast (no x-tilt), 2 fast with x-tilt
   bool xt_common = false;  // every view has the same x-tilt (blended copy for the reprojector)
   float sin_xt_common = 0.0f;
   int fp_variant = 2;  // reprojector variant bits (FpArgs::variant); TG_FP_VARIANT overrides
   float *d_volg = nullptr;  // interleaved copy of the volume for the reprojector
+  size_t volg_elems = 0;
   void *d_volh = nullptr;   // FP16 interleaved copy (half staging forms)
   unsigned *d_maxbits = nullptr;
   int fmt = FMT_ROWPAIR, store = TG_STORE_FP32;
@@ -47,6 +53,7 @@ struct tg_session {  // one tilt series resident on a device
   tg_run_info info{};
   cudaEvent_t ev[6] = {};
   cudaGraphExec_t sirt_exec = nullptr;
+  int iter_launches = 0;  // kernels of one SIRT iteration
   float cx = 0, cz = 0, ocx = 0, inv_n = 0;
   cudaMemPool_t pool = nullptr;  // stream-ordered allocations (server sessions)
   bool dry = false, fail_alloc = false;
@@ -64,6 +71,7 @@ BpArgs bp_args(tg_session *s, int mode);
 FilterArgs filter_args(tg_session *s, bool residual);
 FpArgs fp_args(tg_session *s);
 int launch_bp(tg_session *s, int mode, int *ntiles);
+inline int bp_launch_count(const tg_session *s) { return s->xt_split ? 2 : 1; }
 int autotune(tg_session *s);
 // the tile variant already tuned for this shape (or pinned by TG_BP_VARIANT), else -1
 int tune_lookup(tg_session *s);

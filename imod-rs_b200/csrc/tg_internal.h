@@ -123,6 +123,14 @@ int launch_bp_xtilt(const BpArgs &a, int store, cudaStream_t st, int *ntiles_out
 bool bp_xtilt_supported(int onx, float max_abs_sin_xt, float max_x_extent_per_tile);
 int bp_fast_ntiles(const BpArgs &a, int variant);
 int bp_fast_row_align();  // slices per tile of the widest fast variant
+// Second half of the x-tilt back-projection of a series whose views share one
+// x-tilt: rows holds, per projection row r, the fast kernel's mode-1 output
+// (sum over views of the row-r sample) * 1/N; every voxel (ox, iy) takes rows
+// floor(iy + dx*sin_xt) and the next, blended as the reference blends each
+// view's pair.  a.vol, a.mode (0, 1, 2), a.partial and the output constants as
+// in BpArgs; mode 0 writes XB_TILES partial-stat tiles per slice.
+constexpr int XB_TILES = 64;
+int launch_xt_blend(const BpArgs &a, const float *rows, float sin_xt, cudaStream_t st, int *ntiles_out);
 
 // ---- reprojection (main.rs:831-896) ----
 struct FpArgs {
@@ -143,7 +151,7 @@ struct FpArgs {
                             // bit 2: 32 rows per thread in the half path (else 16);
                             // bit 3: FP32 reprojection also for half staging
 };
-void launch_reproject(const FpArgs &a, cudaStream_t st);
+int launch_reproject(const FpArgs &a, cudaStream_t st);  // returns the kernels launched
 // fills L.table for every (view < nviews, slice < ny, column < onx)
 void launch_local_table(const LocalDev &L, int nviews, int ny, int onx, float2 *table, cudaStream_t st);
 int fp_group_rows(int variant);

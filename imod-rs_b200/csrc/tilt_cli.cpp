@@ -44,6 +44,7 @@ struct Args {
   std::string fill_mode = "mean", cosine_interp = "linear";
   float max_cosine_tilt = 80.0f;
   bool hamming = false;
+  bool exact_xtilt = false;
   long fake_sirt = 0;
   std::string storage = "fp32";
   int device = 0;
@@ -81,6 +82,7 @@ void usage(FILE *f) {
           "      --fake-sirt <N>              Low-pass smoothing passes [default: 0]\n"
           "      --storage <fp32|fp16|bf16>   Staging precision of filtered projections (addition)\n"
           "      --device <N>                 CUDA device ordinal (addition)\n"
+          "      --exact-xtilt                Per-view x-tilt row blend, bit-identical (addition)\n"
           "  -h, --help                       Print help\n\n"
           "PIP-style aliases (additions): -InputProjections -OutputFile -TILTFILE -THICKNESS\n"
           "  -WIDTH -RADIAL -SIRTIterations -LOG -SCALE <add,mult> -FakeSIRTiterations\n"
@@ -125,7 +127,8 @@ Args parse(int argc, char **argv) {
       {"sirtiterations", "sirt"}, {"log", "LOG"}, {"scale", "SCALE"}, {"fakesirtiterations", "fake-sirt"},
       {"xtiltfile", "xtilt-file"}, {"zfactorfile", "zfactor-file"}, {"localfile", "local-file"},
       {"hamming", "hamming"}, {"exactfiltersize", "exact-filter-size"}};
-  const std::vector<std::string> flags = {"gpu", "no-weight", "no-cosine-stretch", "log", "hamming"};
+  const std::vector<std::string> flags = {"gpu", "no-weight", "no-cosine-stretch", "log", "hamming",
+                                          "exact-xtilt"};
   for (int i = 1; i < argc; ++i) {
     std::string arg = argv[i], val;
     bool has_eq = false;
@@ -161,6 +164,7 @@ Args parse(int argc, char **argv) {
       else if (name == "no-cosine-stretch") a.no_cosine_stretch = true;
       else if (name == "log") a.log = true;
       else if (name == "hamming") a.hamming = true;
+      else if (name == "exact-xtilt") a.exact_xtilt = true;
       continue;
     }
     if (!has_eq) {
@@ -306,6 +310,7 @@ int main(int argc, char **argv) {
   o.gpu_compat = args.gpu;
   o.storage = args.storage == "fp16" ? TG_STORE_FP16 : args.storage == "bf16" ? TG_STORE_BF16 : TG_STORE_FP32;
   o.device = args.device;
+  o.exact_xtilt = args.exact_xtilt;
   tg_session *s = nullptr;
   int rc = tg_session_create(&g, &o, &s);
   if (rc == TG_ERR_PANIC) {  // the reference indexes tilt_angles out of bounds and panics

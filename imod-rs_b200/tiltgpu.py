@@ -42,7 +42,8 @@ class Options(C.Structure):
                 ("no_cosine_stretch", _i32), ("cosine_cubic", _i32), ("max_cosine_tilt", _f),
                 ("log_transform", _i32), ("sirt_iters", _i32), ("sirt_relax", _f),
                 ("fake_sirt", _i32), ("densweight", _f), ("outscale", _f), ("outadd", _f),
-                ("gpu_compat", _i32), ("storage", _i32), ("device", _i32), ("use_graphs", _i32)]
+                ("gpu_compat", _i32), ("storage", _i32), ("device", _i32), ("use_graphs", _i32),
+                ("exact_xtilt", _i32)]
 
 
 class Stats(C.Structure):
@@ -205,7 +206,7 @@ def make_options(*, radial=(0.35, 0.05), hamming=False, exact_filter_size=None, 
                  fill_mode="mean", no_cosine_stretch=False, cosine_interp="linear",
                  max_cosine_tilt=80.0, log=False, sirt=0, sirt_relax=1.0, fake_sirt=0,
                  densweight=1.0, outscale=1.0, outadd=0.0, gpu=False, storage="fp32", device=0,
-                 use_graphs=True) -> Options:
+                 use_graphs=True, exact_xtilt=False) -> Options:
     o = Options()
     lib().tg_options_default(C.byref(o))
     o.radial_cutoff, o.radial_falloff = float(radial[0]), float(radial[1])
@@ -222,6 +223,7 @@ def make_options(*, radial=(0.35, 0.05), hamming=False, exact_filter_size=None, 
     o.gpu_compat = int(bool(gpu))
     o.storage = STORAGE[storage] if isinstance(storage, str) else int(storage)
     o.device, o.use_graphs = int(device), int(bool(use_graphs))
+    o.exact_xtilt = int(bool(exact_xtilt))
     return o
 
 
@@ -293,10 +295,11 @@ class Session:
         vals = [_i32() for _ in range(5)]
         check(lib().tg_session_kernel_info(self.h, *[C.byref(v) for v in vals]))
         fast, variant, fmt, padl, pw = (v.value for v in vals)
-        name = {1: None, 2: "xtilt-staged"}.get(fast, "general")
-        return {"fast": fast == 1, "variant": variant,
-                "variant_name": lib().tg_variant_name(variant).decode() if fast == 1 else name,
-                "fmt": fmt, "padL": padl, "PW": pw}
+        name = {2: "xtilt-staged"}.get(fast, "general")
+        if fast in (1, 3):
+            name = lib().tg_variant_name(variant).decode() + ("+xtilt-blend" if fast == 3 else "")
+        return {"fast": fast == 1, "xtilt_split": fast == 3, "variant": variant,
+                "variant_name": name, "fmt": fmt, "padL": padl, "PW": pw}
 
     def set_variant(self, v: int):
         check(lib().tg_session_set_variant(self.h, v))

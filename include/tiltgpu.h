@@ -85,6 +85,10 @@ typedef struct {
   int32_t storage;           /* tg_storage of the staged filtered projections */
   int32_t device;            /* CUDA device ordinal */
   int32_t use_graphs;        /* capture each SIRT iteration in a CUDA graph (1) */
+  int32_t exact_xtilt;       /* x-tilt shared by all views: 0 (default) sums each projection row
+                                over the views, then blends the two rows of every voxel (the
+                                reference's per-view blend up to f32 rounding order); 1 blends
+                                per view, bit-identical to main.rs:802-817 (addition) */
 } tg_options;
 
 /* Output header statistics (amin, amax, amean) of apps/tilt/src/main.rs:1077-1093 */

@@ -28,6 +28,7 @@ def both(proj, ang, precision=32, storage="fp32", **kw):
     okw = dict(kw)
     if "gpu" in okw:
         okw["gpu_compat"] = okw.pop("gpu")
+    okw.pop("exact_xtilt", None)  # a GPU-side choice of summation order
     vol, st = T.reconstruct(proj, ang, storage=storage, **gkw)
     ref, rst = O.run(O.Params(nx, ny, nz, ang, **okw), proj, precision)
     return vol, st, ref, rst
@@ -61,7 +62,7 @@ def test_backprojection_bit_exact_general_xtilt():
     proj = random_stack(nz, ny, nx, seed=4)
     ang = np.linspace(-60, 60, nz).astype(np.float32)
     vol, _, ref, _ = both(proj, ang, no_weight=True, no_cosine_stretch=True,
-                          xtilt=np.full(nz, 1.5, np.float32), thickness=36)
+                          xtilt=np.full(nz, 1.5, np.float32), thickness=36, exact_xtilt=True)
     np.testing.assert_array_equal(vol, ref)
 
 
@@ -81,9 +82,33 @@ def test_backprojection_bit_exact_xtilt_staged(fill, xt, shape):
     else:
         xtv, zf = np.full(nz, xt, np.float32), None
     vol, st, ref, rst = both(proj, ang, no_weight=True, no_cosine_stretch=True, fill_mode=fill,
-                             xtilt=xtv, zfactor=zf, width=onx, thickness=onz)
+                             xtilt=xtv, zfactor=zf, width=onx, thickness=onz, exact_xtilt=True)
     np.testing.assert_array_equal(vol, ref)
     assert st["amin"] == rst["amin"] and st["amax"] == rst["amax"]
+
+
+@pytest.mark.parametrize("fill", ["mean", "zero", "edge"])
+@pytest.mark.parametrize("xt,shape,zf", [(1.5, (15, 21, 70, 75, 37), False), (-8.0, (11, 17, 48, 64, 20), True),
+                                         (0.3, (9, 40, 64, 64, 16), False), (12.0, (7, 9, 40, 33, 50), False)])
+def test_backprojection_xtilt_row_sums(fill, xt, shape, zf):
+    # one x-tilt for all views: the fast kernel sums every projection row over the
+    # views, then each voxel blends its two rows (same rows, fractions, one-row
+    # edges and fills as the reference; only the f32 summation order differs)
+    nz, ny, nx, onx, onz = shape
+    proj = random_stack(nz, ny, nx, seed=nx + onz + 1)
+    ang = np.linspace(-62, 58, nz).astype(np.float32)
+    zfv = np.linspace(0.9, 1.2, nz).astype(np.float32) if zf else None
+    kw = dict(no_weight=True, no_cosine_stretch=True, fill_mode=fill, xtilt=np.full(nz, xt, np.float32),
+              zfactor=zfv, width=onx, thickness=onz)
+    with T.Session(nx, ny, nz, ang, **kw) as s:
+        info = s.kernel_info()
+    assert info["xtilt_split"], info
+    vol, st, ref, rst = both(proj, ang, **kw)
+    assert rel_l2(vol, ref) <= 1e-6
+    assert np.abs(vol - ref).max() <= 1e-5 * max(1.0, float(np.abs(ref).max()))
+    assert abs(st["amin"] - rst["amin"]) <= 1e-5 and abs(st["amax"] - rst["amax"]) <= 1e-5
+    exact, _, _, _ = both(proj, ang, exact_xtilt=True, **kw)
+    np.testing.assert_array_equal(exact, ref)
 
 
 def test_backprojection_bit_exact_local_alignment():
