@@ -289,14 +289,18 @@ __device__ __forceinline__ void acc2_f16(float &a0, float &a1, uint32_t h2) {
       : "r"(h2));
 }
 
+// Power-of-two scale of the FP16 copy: copied values stay below 2^9, so the
+// half-precision partial sums of fp_half_kernel (at most HALF_FLUSH depths, each
+// at most (1/0.05 + 1) = 21 weighted values) stay below 2^9 * 42 < 65504.
 // headroom: 1 when the copied values are blends of two slices (|b| < 2 max|v|)
+constexpr int HALF_FLUSH = 2;
 __device__ __forceinline__ float half_scale(const unsigned *maxbits, bool inverse, int headroom = 0) {
   const float m = __uint_as_float(*maxbits);
   if (!(m > 0.0f) || !(m < 3.0e38f)) return 1.0f;
   int e;
   frexpf(m, &e);  // m < 2^e
   e += headroom;
-  return inverse ? ldexpf(1.0f, e - 14) : ldexpf(1.0f, 14 - e);
+  return inverse ? ldexpf(1.0f, e - 9) : ldexpf(1.0f, 9 - e);
 }
 
 __global__ void absmax_kernel(const float *__restrict__ vol, size_t n, unsigned *maxbits) {
@@ -362,6 +366,11 @@ __global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
   float acc[S];
 #pragma unroll
   for (int s = 0; s < S; ++s) acc[s] = 0.0f;
+  // FP16 partial sums over HALF_FLUSH depths (packed fma), folded into the FP32
+  // accumulators with mixed-precision adds
+  __half2 ph[S / 2];
+#pragma unroll
+  for (int m = 0; m < S / 2; ++m) ph[m] = __float2half2_rn(0.0f);
   // Tolerance path: x(ox) = ox*c + c0 with one FMA (within a few ulp of the reference's
   // ((dx*cos)*cos_xt + t2) + cx, and non-decreasing in ox, which the search needs)
   const float c = XT ? cos_t * cos_xt : cos_t;
@@ -394,10 +403,15 @@ __global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
         const uint4 u = __ldg(q + k);
         const uint32_t uu[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          const __half2 prod = __hmul2(*reinterpret_cast<const __half2 *>(&uu[m]), w2);
-          acc2_f16(acc[8 * k + 2 * m], acc[8 * k + 2 * m + 1], *reinterpret_cast<const uint32_t *>(&prod));
-        }
+        for (int m = 0; m < 4; ++m)
+          ph[4 * k + m] = __hfma2(*reinterpret_cast<const __half2 *>(&uu[m]), w2, ph[4 * k + m]);
+      }
+    }
+    if ((oz + 1) % HALF_FLUSH == 0 || oz + 1 == a.onz) {
+#pragma unroll
+      for (int m = 0; m < S / 2; ++m) {
+        acc2_f16(acc[2 * m], acc[2 * m + 1], *reinterpret_cast<const uint32_t *>(&ph[m]));
+        ph[m] = __float2half2_rn(0.0f);
       }
     }
   }
