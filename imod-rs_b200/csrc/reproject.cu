@@ -275,12 +275,13 @@ __global__ void interleave_kernel(const float *__restrict__ vol, float *__restri
 
 // ---- half-precision reprojection (FP16/BF16 staging forms) ----
 // The volume is copied into the row-group-interleaved layout as FP16 scaled by a
-// power of two 2^(14-e), where max|v| < 2^e, so the largest value stays below
-// 2^14 and no value overflows; the scale is exact and undone on the sums.  A
-// column visit then loads S halves in S/8 16-byte loads, forms the products
-// with packed half multiplies and accumulates them in FP32 (mixed-precision
-// add).  Tolerance path: each volume value and product carries a relative
-// rounding of 2^-11 and the accumulation stays FP32.
+// power of two 2^(9-e), where max|v| < 2^e, so every value stays below 2^9 and
+// the half partial sums below have headroom; the scale is exact and undone on
+// the sums.  A column visit loads S halves in S/8 16-byte loads and adds the
+// weighted values to packed half partial sums (fma), which are folded into the
+// FP32 accumulators (mixed-precision add) every HALF_FLUSH depths.  Tolerance
+// path: each volume value and partial sum carries a relative rounding of
+// 2^-11; the accumulation over depths stays FP32.
 
 __device__ __forceinline__ void acc2_f16(float &a0, float &a1, uint32_t h2) {
   asm("{\n .reg .f16 lo, hi;\n mov.b32 {lo, hi}, %2;\n"
