@@ -131,15 +131,16 @@ template <int I, int N, class F> __device__ __forceinline__ void static_for(F &&
 constexpr float MAGIC = 12582912.0f;      // 1.5 * 2^23
 constexpr uint32_t MAGIC_BITS = 0x4B400000u;
 
-// exact reference position for (dx, dz): ((dx*c)*cxt + (dz*s)*zf) + cx
-template <bool ZF>
+// exact reference position for (dx, dz): ((dx*c)*cxt + (dz*s)*zf) + cx.
+// ZF: 0 no z-factor, 1 z-factor, 2 z-factor and x-tilt (t1 carries *cos_xt)
+template <int ZF>
 __device__ __forceinline__ float ref_x(float t1, float dz, float s, float zf, float cx) {
   float t2 = __fmul_rn(dz, s);
   if (ZF) t2 = __fmul_rn(t2, zf);
   return __fadd_rn(__fadd_rn(t1, t2), cx);
 }
 
-template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
 struct FastCfg {
   static constexpr int SP = S / 2;           // row pairs per tile
   static constexpr int OZG = NT / TX;        // depth groups of consumer threads
@@ -213,7 +214,7 @@ template <class C> struct SmemLayout {
 // One output tile (S slices x TX columns x TZ depths) of one series.  gst is the
 // CTA's running stage count: ring slots and mbarrier phases continue across the
 // tiles a persistent CTA processes.  Returns false on abort.
-template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
 __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz, unsigned char *sm,
                                         const SmemLayout<FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>> &L,
                                         int &gst, volatile int *s_abort_p) {
@@ -232,8 +233,12 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
   // ---- per-view windows of this tile (x is monotone in dx and dz: corners bound it)
   for (int v = tid; v < a.nviews; v += C::NTHR) {
     float4 g = __ldg(&a.vg[v]);
-    float t1l = __fmul_rn(__fmul_rn(__fsub_rn((float)oxlo, a.ocx), g.x), g.w);
-    float t1h = __fmul_rn(__fmul_rn(__fsub_rn((float)oxhi, a.ocx), g.x), g.w);
+    float t1l = __fmul_rn(__fsub_rn((float)oxlo, a.ocx), g.x);
+    float t1h = __fmul_rn(__fsub_rn((float)oxhi, a.ocx), g.x);
+    if (ZF == 2) {  // x-tilt: (dx*cos_t)*cos_xt
+      t1l = __fmul_rn(t1l, g.w);
+      t1h = __fmul_rn(t1h, g.w);
+    }
     float dzl = __fsub_rn((float)ozlo, a.cz), dzh = __fsub_rn((float)ozhi, a.cz);
     float x0 = ref_x<ZF>(t1l, dzl, g.y, g.z, a.cx), x1 = ref_x<ZF>(t1l, dzh, g.y, g.z, a.cx);
     float x2 = ref_x<ZF>(t1h, dzl, g.y, g.z, a.cx), x3 = ref_x<ZF>(t1h, dzh, g.y, g.z, a.cx);
@@ -329,8 +334,8 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
       if (vi < nv) {
         const int v = v0 + vi;
         const float4 g = __ldg(&a.vg[v]);
-        // (dx*cos_t)*cos_xt; cos_xt is 1 exactly without x-tilt (the product is then dx*cos_t)
-        const float t1 = __fmul_rn(__fmul_rn(dx, g.x), g.w);
+        // (dx*cos_t)*cos_xt; without x-tilt (ZF < 2) cos_xt is 1 and the product dx*cos_t
+        const float t1 = ZF == 2 ? __fmul_rn(__fmul_rn(dx, g.x), g.w) : __fmul_rn(dx, g.x);
         // half staging (a tolerance path): one FMA per position, x within an ulp of the
         // reference's; linear interpolation is continuous, so a floor moved by it
         // changes the sample by at most the rounding of x
@@ -485,7 +490,7 @@ template <class C> __device__ __forceinline__ void drain_ring(const SmemLayout<C
 }
 
 // One launch per series: grid = tiles of that series.
-template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
 __global__ void __launch_bounds__(NT + 32) bp_fast_kernel(const __grid_constant__ BpArgs a) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   extern __shared__ __align__(128) unsigned char sm[];
@@ -501,7 +506,7 @@ __global__ void __launch_bounds__(NT + 32) bp_fast_kernel(const __grid_constant_
 // tile of the queue (longest series first) until it is empty.  Each tile's
 // arithmetic is the same as in the per-series kernel, so every series' result
 // does not depend on what else is in the batch.
-template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
 __global__ void __launch_bounds__(NT + 32) bp_batch_kernel(const BpArgs *__restrict__ jobs, int njobs,
                                                            int ntiles, int *counter, int max_views) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
@@ -564,7 +569,7 @@ int bp_fast_variants() { return (int)(sizeof(kFast) / sizeof(kFast[0])); }
 const char *bp_fast_variant_name(int v) { return kFast[v].name; }
 int bp_fast_row_align() { return MAX_S; }
 
-template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
 static int launch_fast_t(const BpArgs &a0, cudaStream_t st, int *ntiles) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   auto kern = bp_fast_kernel<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
@@ -581,7 +586,7 @@ static int launch_fast_t(const BpArgs &a0, cudaStream_t st, int *ntiles) {
   return TG_OK;
 }
 
-template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, bool ZF>
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
 static int launch_batch_t(const BatchLaunch &bl, cudaStream_t st) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   auto kern = bp_batch_kernel<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
@@ -601,7 +606,7 @@ static int launch_batch_t(const BatchLaunch &bl, cudaStream_t st) {
   return TG_OK;
 }
 
-template <int STORE, bool ZF>
+template <int STORE, int ZF>
 static int launch_fast_v(const BpArgs &a, int variant, cudaStream_t st, int *ntiles) {
   switch (variant) {
     case 0: return launch_fast_t<STORE, 8, 4, 32, 128, 2, 4, ZF>(a, st, ntiles);
@@ -619,7 +624,7 @@ static int launch_fast_v(const BpArgs &a, int variant, cudaStream_t st, int *nti
   }
 }
 
-template <int STORE, bool ZF>
+template <int STORE, int ZF>
 static int launch_batch_v(const BatchLaunch &bl, int variant, cudaStream_t st) {
   switch (variant) {
     case 0: return launch_batch_t<STORE, 8, 4, 32, 128, 2, 4, ZF>(bl, st);
@@ -640,10 +645,10 @@ static int launch_batch_v(const BatchLaunch &bl, int variant, cudaStream_t st) {
 int launch_bp_batch(const BatchLaunch &bl, int store, bool zf, int variant, cudaStream_t st) {
   if (variant < 0 || variant >= bp_fast_variants()) variant = 0;
   if (store == TG_STORE_FP32)
-    return zf ? launch_batch_v<TG_STORE_FP32, true>(bl, variant, st) : launch_batch_v<TG_STORE_FP32, false>(bl, variant, st);
+    return zf ? launch_batch_v<TG_STORE_FP32, 1>(bl, variant, st) : launch_batch_v<TG_STORE_FP32, 0>(bl, variant, st);
   if (store == TG_STORE_FP16)
-    return zf ? launch_batch_v<TG_STORE_FP16, true>(bl, variant, st) : launch_batch_v<TG_STORE_FP16, false>(bl, variant, st);
-  return zf ? launch_batch_v<TG_STORE_BF16, true>(bl, variant, st) : launch_batch_v<TG_STORE_BF16, false>(bl, variant, st);
+    return zf ? launch_batch_v<TG_STORE_FP16, 1>(bl, variant, st) : launch_batch_v<TG_STORE_FP16, 0>(bl, variant, st);
+  return zf ? launch_batch_v<TG_STORE_BF16, 1>(bl, variant, st) : launch_batch_v<TG_STORE_BF16, 0>(bl, variant, st);
 }
 
 void bp_fast_tile_shape(int variant, int *S, int *TX, int *TZ) {
@@ -659,16 +664,17 @@ int bp_fast_ntiles(const BpArgs &a, int variant) {
   return ((a.onx + f.TX - 1) / f.TX) * ((a.onz + tz - 1) / tz);
 }
 
-int launch_bp_fast(const BpArgs &a, int store, bool zf, int variant, cudaStream_t st, int *ntiles) {
+template <int STORE>
+static int launch_fast_z(const BpArgs &a, int zf, int variant, cudaStream_t st, int *ntiles) {
+  return zf == 2 ? launch_fast_v<STORE, 2>(a, variant, st, ntiles)
+                 : zf ? launch_fast_v<STORE, 1>(a, variant, st, ntiles) : launch_fast_v<STORE, 0>(a, variant, st, ntiles);
+}
+
+int launch_bp_fast(const BpArgs &a, int store, int zf, int variant, cudaStream_t st, int *ntiles) {
   if (variant < 0 || variant >= bp_fast_variants()) variant = 0;
-  if (store == TG_STORE_FP32)
-    return zf ? launch_fast_v<TG_STORE_FP32, true>(a, variant, st, ntiles)
-              : launch_fast_v<TG_STORE_FP32, false>(a, variant, st, ntiles);
-  if (store == TG_STORE_FP16)
-    return zf ? launch_fast_v<TG_STORE_FP16, true>(a, variant, st, ntiles)
-              : launch_fast_v<TG_STORE_FP16, false>(a, variant, st, ntiles);
-  return zf ? launch_fast_v<TG_STORE_BF16, true>(a, variant, st, ntiles)
-            : launch_fast_v<TG_STORE_BF16, false>(a, variant, st, ntiles);
+  if (store == TG_STORE_FP32) return launch_fast_z<TG_STORE_FP32>(a, zf, variant, st, ntiles);
+  if (store == TG_STORE_FP16) return launch_fast_z<TG_STORE_FP16>(a, zf, variant, st, ntiles);
+  return launch_fast_z<TG_STORE_BF16>(a, zf, variant, st, ntiles);
 }
 
 // ---------------------------------------------------------------------------

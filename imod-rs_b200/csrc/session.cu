@@ -303,11 +303,11 @@ FilterArgs filter_args(tg_session *s, bool residual) {
 
 int launch_bp(tg_session *s, int mode, int *ntiles) {
   BpArgs a = bp_args(s, mode);
-  if (s->fast) return launch_bp_fast(a, s->store, s->zf_any, s->variant < 0 ? 0 : s->variant, s->st, ntiles);
+  if (s->fast) return launch_bp_fast(a, s->store, fast_zf(s), s->variant < 0 ? 0 : s->variant, s->st, ntiles);
   if (s->xt_split) {  // per-row view sums, then the two-row blend of every voxel
     BpArgs r = bp_args(s, 1);
     r.vol = s->xtb;
-    int rc = launch_bp_fast(r, s->store, s->zf_any, s->variant < 0 ? 0 : s->variant, s->st, nullptr);
+    int rc = launch_bp_fast(r, s->store, fast_zf(s), s->variant < 0 ? 0 : s->variant, s->st, nullptr);
     if (rc != TG_OK) return rc;
     return launch_xt_blend(a, s->xtb, s->sin_xt_common, s->st, ntiles);
   }
@@ -323,7 +323,7 @@ int autotune(tg_session *s) {
     int v = atoi(env);
     if (v >= 0 && v < bp_fast_variants()) { s->variant = v; return TG_OK; }
   }
-  auto key = std::make_tuple(s->nx, s->onx, s->onz, s->nviews, s->store, (int)s->zf_any, s->ny >= 64 ? 64 : s->ny);
+  auto key = std::make_tuple(s->nx, s->onx, s->onz, s->nviews, s->store, fast_zf(s), s->ny >= 64 ? 64 : s->ny);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(key);
@@ -339,9 +339,9 @@ int autotune(tg_session *s) {
     if (s->xt_split) a.vol = s->xtb;
     int nt = 0;
     // warm + timed launch (mode 1 writes the volume, which is rewritten afterwards)
-    if (launch_bp_fast(a, s->store, s->zf_any, v, s->st, &nt) != TG_OK) continue;
+    if (launch_bp_fast(a, s->store, fast_zf(s), v, s->st, &nt) != TG_OK) continue;
     cudaEventRecord(e0, s->st);
-    launch_bp_fast(a, s->store, s->zf_any, v, s->st, &nt);
+    launch_bp_fast(a, s->store, fast_zf(s), v, s->st, &nt);
     cudaEventRecord(e1, s->st);
     if (cudaEventSynchronize(e1) != cudaSuccess) break;
     float ms = 0;
@@ -363,7 +363,7 @@ int tune_lookup(tg_session *s) {
     int v = atoi(env);
     if (v >= 0 && v < bp_fast_variants()) return v;
   }
-  auto key = std::make_tuple(s->nx, s->onx, s->onz, s->nviews, s->store, (int)s->zf_any, s->ny >= 64 ? 64 : s->ny);
+  auto key = std::make_tuple(s->nx, s->onx, s->onz, s->nviews, s->store, fast_zf(s), s->ny >= 64 ? 64 : s->ny);
   std::lock_guard<std::mutex> lk(g_tune_mu);
   auto it = g_tune.find(key);
   return it != g_tune.end() ? it->second : -1;

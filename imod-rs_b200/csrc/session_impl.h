@@ -72,6 +72,8 @@ FilterArgs filter_args(tg_session *s, bool residual);
 FpArgs fp_args(tg_session *s);
 int launch_bp(tg_session *s, int mode, int *ntiles);
 inline int bp_launch_count(const tg_session *s) { return s->xt_split ? 2 : 1; }
+// position form of the fast kernel: 2 with x-tilt (row sums), else whether z-factors apply
+inline int fast_zf(const tg_session *s) { return s->xt_split ? 2 : s->zf_any ? 1 : 0; }
 int autotune(tg_session *s);
 // the tile variant already tuned for this shape (or pinned by TG_BP_VARIANT), else -1
 int tune_lookup(tg_session *s);

@@ -109,7 +109,8 @@ int launch_bp_batch(const BatchLaunch &bl, int store, bool zf, int variant, cuda
 void bp_fast_tile_shape(int variant, int *S, int *TX, int *TZ);
 struct BpTile { int S, K, TX, NT, VPS, wmax; };
 // Fast kernel: no x-tilt, no local alignment, ROWPAIR format.
-int launch_bp_fast(const BpArgs &a, int store, bool zf, int variant, cudaStream_t st,
+// zf: 0 none, 1 z-factors, 2 z-factors and one x-tilt in the positions (row sums)
+int launch_bp_fast(const BpArgs &a, int store, int zf, int variant, cudaStream_t st,
                    int *ntiles_out);
 int bp_fast_variants();
 const char *bp_fast_variant_name(int v);
