@@ -177,16 +177,17 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
       const float frac = __fsub_rn(x, __fsub_rn(tt, FMAGIC));
       const float w = x0 == p ? __fsub_rn(1.0f, frac) : frac;
       if (IL) {
-        // interleaved copy: the S rows of this row group at (oz, ox) are contiguous; with
+        // interleaved copy: the S rows of this row group at (oz, ox) are S/4 float4s, one
+        // per 4-row plane (neighbouring threads' columns are neighbouring float4s); with
         // x-tilt each holds the row's blend of its two source slices (blend_interleave_kernel)
         const float4 *q = reinterpret_cast<const float4 *>(a.volg) +
-                          (((size_t)blockIdx.z * a.onz + oz) * a.onx + ox) * (S / 4);
+                          ((size_t)blockIdx.z * a.onz + oz) * a.onx * (S / 4) + ox;
         // products on the f32x2 pipe; the sums stay scalar so that no product is
         // contracted into them (each stays RN(acc + RN(v*w)), the reference's operations)
         const uint64_t w2 = pk2(w, w);
 #pragma unroll
         for (int k = 0; k < S / 4; ++k) {
-          const float4 q4 = __ldg(q + k);
+          const float4 q4 = __ldg(q + (size_t)k * a.onx);
           const float2 pa = up2(mul2(pk2(q4.x, q4.y), w2)), pb = up2(mul2(pk2(q4.z, q4.w), w2));
           acc[4 * k + 0] = __fadd_rn(acc[4 * k + 0], pa.x);
           acc[4 * k + 1] = __fadd_rn(acc[4 * k + 1], pa.y);
@@ -254,7 +255,8 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
     if (s < nrows) a.sino[((size_t)v * a.ny + r0 + s) * a.nx + p] = acc[s];
 }
 
-// volg[g][oz][ox][j] = vol[g*G + j][oz][ox] (zero for rows past ny)
+// volg[g][oz][j/4][ox][j%4] = vol[g*G + j][oz][ox] (zero for rows past ny): per
+// (row group, depth) G/4 planes of float4s, each plane a row of columns
 template <int G>
 __global__ void interleave_kernel(const float *__restrict__ vol, float *__restrict__ volg, int ny,
                                   int onz, int onx, size_t n) {
@@ -268,9 +270,11 @@ __global__ void interleave_kernel(const float *__restrict__ vol, float *__restri
     const size_t iy = g * G + j;
     v[j] = iy < (size_t)ny ? __ldg(vol + iy * sl + rem) : 0.0f;
   }
-  float4 *o = reinterpret_cast<float4 *>(volg) + i * (G / 4);
+  const size_t ox = rem % onx;
+  float4 *o = reinterpret_cast<float4 *>(volg) + (i - ox) * (G / 4) + ox;
 #pragma unroll
-  for (int k = 0; k < G / 4; ++k) o[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+  for (int k = 0; k < G / 4; ++k)
+    o[(size_t)k * onx] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
 }
 
 // ---- half-precision reprojection (FP16/BF16 staging forms) ----
@@ -326,7 +330,7 @@ __global__ void absmax_kernel(const float *__restrict__ vol, size_t n, unsigned 
   if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(maxbits, __float_as_uint(m));  // |v| orders as its bits
 }
 
-// volh[g][oz][ox][j] = half(vol[g*G + j][oz][ox] * scale) (zero past ny)
+// volh[g][oz][j/8][ox][j%8] = half(vol[g*G + j][oz][ox] * scale) (zero past ny)
 template <int G>
 __global__ void interleave_half_kernel(const float *__restrict__ vol, __half *__restrict__ volh, int ny,
                                        int onz, int onx, size_t n, const unsigned *maxbits) {
@@ -344,9 +348,11 @@ __global__ void interleave_half_kernel(const float *__restrict__ vol, __half *__
     const __half2 h = __floats2half2_rn(v0, v1);
     w[j / 2] = *reinterpret_cast<const uint32_t *>(&h);
   }
-  uint4 *o = reinterpret_cast<uint4 *>(volh) + i * (G / 8);
+  const size_t ox = rem % onx;
+  uint4 *o = reinterpret_cast<uint4 *>(volh) + (i - ox) * (G / 8) + ox;
 #pragma unroll
-  for (int k = 0; k < G / 8; ++k) o[k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
+  for (int k = 0; k < G / 8; ++k)
+    o[(size_t)k * onx] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
 }
 
 template <int S, bool XT>
@@ -398,10 +404,10 @@ __global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
       if ((unsigned)x0 > (unsigned)(a.nx - 2)) continue;
       const float frac = __fsub_rn(x, __fsub_rn(tt, FMAGIC));
       const __half2 w2 = __float2half2_rn(x0 == p ? __fsub_rn(1.0f, frac) : frac);
-      const uint4 *q = vz + (size_t)ox * (S / 8);
+      const uint4 *q = vz + ox;  // plane k of this column at q + k*onx
 #pragma unroll
       for (int k = 0; k < S / 8; ++k) {
-        const uint4 u = __ldg(q + k);
+        const uint4 u = __ldg(q + (size_t)k * a.onx);
         const uint32_t uu[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
         for (int m = 0; m < 4; ++m)
@@ -469,9 +475,10 @@ __global__ void blend_interleave_kernel(const float *__restrict__ vol, float *__
   float b[G];
 #pragma unroll
   for (int j = 0; j < G; ++j) b[j] = blend_row(vol, ny, sl, rem, (int)g * G + j, nn, yoff, two_ok);
-  float4 *o = reinterpret_cast<float4 *>(volb) + i * (G / 4);
+  float4 *o = reinterpret_cast<float4 *>(volb) + (i - (size_t)ox) * (G / 4) + ox;  // layout of interleave_kernel
 #pragma unroll
-  for (int k = 0; k < G / 4; ++k) o[k] = make_float4(b[4 * k], b[4 * k + 1], b[4 * k + 2], b[4 * k + 3]);
+  for (int k = 0; k < G / 4; ++k)
+    o[(size_t)k * onx] = make_float4(b[4 * k], b[4 * k + 1], b[4 * k + 2], b[4 * k + 3]);
 }
 
 // The same blend into the scaled FP16 copy of the half-staging forms (a blend of
@@ -497,9 +504,10 @@ __global__ void blend_interleave_half_kernel(const float *__restrict__ vol, __ha
                                         blend_row(vol, ny, sl, rem, r + 1, nn, yoff, two_ok) * sc);
     w[j / 2] = *reinterpret_cast<const uint32_t *>(&h);
   }
-  uint4 *o = reinterpret_cast<uint4 *>(volh) + i * (G / 8);
+  uint4 *o = reinterpret_cast<uint4 *>(volh) + (i - (size_t)ox) * (G / 8) + ox;  // layout of interleave_half_kernel
 #pragma unroll
-  for (int k = 0; k < G / 8; ++k) o[k] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
+  for (int k = 0; k < G / 8; ++k)
+    o[(size_t)k * onx] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
 }
 
 template <int S>
