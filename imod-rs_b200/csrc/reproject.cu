@@ -165,11 +165,11 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
     lo = min(max(lo, 0), a.onx);
     float flo = (float)lo;
     while (lo > 0 && X(flo - 1.0f, t2) >= lo_t) { --lo; flo -= 1.0f; }
-    while (lo < a.onx && X(flo, t2) < lo_t) { ++lo; flo += 1.0f; }
+    float x = X(flo, t2);  // carried into the visit loop: each position is evaluated once
+    while (lo < a.onx && x < lo_t) { ++lo; flo += 1.0f; x = X(flo, t2); }
     const float *vz = a.vol + (size_t)oz * a.onx;
     float fo = flo;
-    for (int ox = lo; ox < a.onx; ++ox, fo += 1.0f) {
-      const float x = X(fo, t2);
+    for (int ox = lo; ox < a.onx; ++ox, fo += 1.0f, x = X(fo, t2)) {
       if (!(x < hi_t)) break;
       const float tt = __fadd_rd(x, FMAGIC);
       const int x0 = (int)(__float_as_uint(tt) - FMAGIC_BITS);
@@ -393,11 +393,11 @@ __global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
     lo = min(max(lo, 0), a.onx);
     float flo = (float)lo;
     while (lo > 0 && X(flo - 1.0f) >= lo_t) { --lo; flo -= 1.0f; }
-    while (lo < a.onx && X(flo) < lo_t) { ++lo; flo += 1.0f; }
+    float x = X(flo);  // carried into the visit loop
+    while (lo < a.onx && x < lo_t) { ++lo; flo += 1.0f; x = X(flo); }
     const uint4 *vz = vg + (size_t)oz * a.onx * (S / 8);
     float fo = flo;
-    for (int ox = lo; ox < a.onx; ++ox, fo += 1.0f) {
-      const float x = X(fo);
+    for (int ox = lo; ox < a.onx; ++ox, fo += 1.0f, x = X(fo)) {
       if (!(x < hi_t)) break;
       const float tt = __fadd_rd(x, FMAGIC);
       const int x0 = (int)(__float_as_uint(tt) - FMAGIC_BITS);
