@@ -18,6 +18,14 @@ def test_help():
     assert r.returncode == 0 and "--tilt-file" in r.stdout and "--fake-sirt" in r.stdout
 
 
+def test_exact_xtilt_flag():
+    r = run("--help")
+    assert "--exact-xtilt" in r.stdout
+    # a flag takes no value
+    r = run("-i", "a", "-o", "b", "-t", "c", "--exact-xtilt=1")
+    assert r.returncode == 2 and "exact-xtilt" in r.stderr
+
+
 def test_missing_required_arguments():
     r = run("-i", "a.mrc")
     assert r.returncode == 2 and "--output" in r.stderr and "--tilt-file" in r.stderr
