@@ -295,10 +295,10 @@ __device__ __forceinline__ void acc2_f16(float &a0, float &a1, uint32_t h2) {
 }
 
 // Power-of-two scale of the FP16 copy: copied values stay below 2^9, so the
-// half-precision partial sums of fp_half_kernel (at most HALF_FLUSH depths, each
-// at most (1/0.05 + 1) = 21 weighted values) stay below 2^9 * 42 < 65504.
+// half-precision partial sums of fp_half_kernel (HALF_FLUSH = 4 depths, each
+// adding weights that sum to at most 1/0.05 + 1 = 21) stay below 2^9 * 84 < 65504.
 // headroom: 1 when the copied values are blends of two slices (|b| < 2 max|v|)
-constexpr int HALF_FLUSH = 2;
+constexpr int HALF_FLUSH = 4;
 __device__ __forceinline__ float half_scale(const unsigned *maxbits, bool inverse, int headroom = 0) {
   const float m = __uint_as_float(*maxbits);
   if (!(m > 0.0f) || !(m < 3.0e38f)) return 1.0f;
