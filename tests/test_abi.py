@@ -40,6 +40,19 @@ def test_abi_version_and_defaults():
     assert T.lib().tg_status_string(-8) == b"input on which the reference panics"
 
 
+def test_options_struct_matches_header():
+    # tg_options_default clears the whole C struct: a sentinel right after the
+    # Python mirror must survive (the mirror is not shorter than the C struct),
+    # and the last field (exact_xtilt) defaults to 0 with use_graphs on
+    n = C.sizeof(T.Options)
+    buf = (C.c_ubyte * (n + 32))(*([0xA5] * (n + 32)))
+    T.lib().tg_options_default(C.cast(buf, C.POINTER(T.Options)))
+    assert bytes(buf[n:]) == b"\xa5" * 32
+    o = T.Options.from_buffer_copy(bytes(buf[:n]))
+    assert o.use_graphs == 1 and o.exact_xtilt == 0
+    assert T.make_options(exact_xtilt=True).exact_xtilt == 1
+
+
 def test_session_without_gpu_fails_loudly():
     try:
         import torch
