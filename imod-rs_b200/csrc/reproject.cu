@@ -609,19 +609,25 @@ __global__ void __launch_bounds__(128) fp_local_kernel(FpArgs a) {
     const float t2 = __fmul_rn(__fmul_rn(dz, sin_t), zf);
     int lo = 0, hi = a.onx - 1;
     if (inv_a != 0.0f) {
+      // columns whose corrected position xb + dx_local can lie in [p-1, p+1) with
+      // |dx_local| <= lxmax; the margin (0.05 px, in columns, plus 1e-3 column) covers
+      // the f32 rounding of the positions (a few ulp of values below 2^14) and of 1/a
       const float base = a.cx + t2;
       const float d1 = (pf - 1.0f - lxmax - base) * inv_a, d2 = (pf + 1.0f + lxmax - base) * inv_a;
-      const float dmin = fmaxf(fminf(d1, d2) + a.ocx, -1.0f), dmax = fminf(fmaxf(d1, d2) + a.ocx, (float)a.onx);
-      lo = max((int)floorf(dmin) - 1, 0);
-      hi = min((int)ceilf(dmax) + 1, a.onx - 1);
+      const float m = 0.05f * fabsf(inv_a) + 1e-3f;
+      const float dmin = fmaxf(fminf(d1, d2) + a.ocx - m, -1.0f), dmax = fminf(fmaxf(d1, d2) + a.ocx + m, (float)a.onx);
+      lo = max((int)ceilf(dmin), 0);
+      hi = min((int)floorf(dmax), a.onx - 1);
     }
     for (int ox = lo; ox <= hi; ++ox) {
       const float dx = __fsub_rn((float)ox, a.ocx);
       const float xb = __fadd_rn(__fadd_rn(__fmul_rn(__fmul_rn(dx, cos_t), cos_xt), t2), a.cx);
       const float yoff = __fmul_rn(dx, sin_xt);
-      // slices whose corrected row can reach rows [r0, r0 + nrows)
-      const int iy_lo = max((int)floorf((float)r0 - 2.0f - yoff - lymax), 0);
-      const int iy_hi = min((int)ceilf((float)(r0 + nrows) + 1.0f - yoff + lymax), a.ny - 1);
+      // slices whose corrected row iy + yoff + dy_local (|dy_local| <= lymax) lies in
+      // [r0 - 1, r0 + nrows): the rows [r0, r0 + nrows) receive from floor rows r0-1 ..
+      // r0+nrows-1; margin 0.01 row for rounding
+      const int iy_lo = max((int)ceilf((float)r0 - 1.0f - yoff - lymax - 0.01f), 0);
+      const int iy_hi = min((int)floorf((float)(r0 + nrows) - yoff + lymax + 0.01f), a.ny - 1);
       for (int iy = iy_lo; iy <= iy_hi; ++iy) {
         const float2 l = __ldg(&a.loc.table[((size_t)v * a.ny + iy) * a.loc.table_nx + ox]);
         const float x = __fadd_rn(xb, l.x);
