@@ -574,6 +574,34 @@ void launch_local_table(const LocalDev &L, int nviews, int ny, int onx, float2 *
   local_table_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(L, nviews, ny, onx, table);
 }
 
+// dx range of the corrections per (view, slice tile t, column) over the slices that a
+// reprojection block of row group t can read when the x-tilt and dy shifts stay
+// within one tile: [LB_TILE*(t-1), LB_TILE*(t+2)) clipped to [0, ny)
+__global__ void local_bounds_kernel(const float2 *__restrict__ table, int nviews, int ny, int onx, int ntile,
+                                    float2 *bnd) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (v, t, ox)
+  const size_t n = (size_t)nviews * ntile * onx;
+  if (i >= n) return;
+  const int ox = (int)(i % onx);
+  const size_t r = i / onx;
+  const int t = (int)(r % ntile), v = (int)(r / ntile);
+  const int y0 = max(LB_TILE * (t - 1), 0), y1 = min(LB_TILE * (t + 2), ny);
+  float mn = 3.40282347e+38f, mx = -3.40282347e+38f;
+  for (int iy = y0; iy < y1; ++iy) {
+    const float d = __ldg(&table[((size_t)v * ny + iy) * onx + ox]).x;
+    mn = fminf(mn, d);
+    mx = fmaxf(mx, d);
+  }
+  bnd[i] = make_float2(mn, mx);
+}
+
+void launch_local_bounds(const float2 *table, int nviews, int ny, int onx, float2 *bnd, cudaStream_t st) {
+  const int ntile = (ny + LB_TILE - 1) / LB_TILE;
+  const size_t n = (size_t)nviews * ntile * onx;
+  if (n == 0) return;
+  local_bounds_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(table, nviews, ny, onx, ntile, bnd);
+}
+
 // Reprojection with local alignment: one thread owns bin p of S (16) rows of one view
 // and gathers, per depth, every (column, slice) whose corrected position lands
 // in [p-1, p+1) and whose corrected row reaches one of its rows, with the
@@ -583,6 +611,7 @@ void launch_local_table(const LocalDev &L, int nviews, int ny, int onx, float2 *
 // target row depends on the slice's correction).  Order: z, x, slice.
 template <int S>
 __global__ void __launch_bounds__(128) fp_local_kernel(FpArgs a) {
+  static_assert(S == LB_TILE, "row groups are the slice tiles of FpArgs::lbnd");
   __shared__ float sacc[S][128];
   const int tid = threadIdx.x;
   const int v = blockIdx.x;
@@ -628,6 +657,13 @@ __global__ void __launch_bounds__(128) fp_local_kernel(FpArgs a) {
       // r0+nrows-1; margin 0.01 row for rounding
       const int iy_lo = max((int)ceilf((float)r0 - 1.0f - yoff - lymax - 0.01f), 0);
       const int iy_hi = min((int)floorf((float)(r0 + nrows) - yoff + lymax + 0.01f), a.ny - 1);
+      // skip the column when no slice of the window can land in [p-1, p+1): f32 addition
+      // is monotone, so xb + dx lies in [RN(xb + dx_min), RN(xb + dx_max)] for every slice
+      // whose dx the tile bound covers
+      if (a.lbnd && iy_lo >= max(r0 - LB_TILE, 0) && iy_hi < min(r0 + 2 * LB_TILE, a.ny)) {
+        const float2 b = __ldg(&a.lbnd[((size_t)v * gridDim.z + blockIdx.z) * a.onx + ox]);
+        if (__fadd_rn(xb, b.y) < pf - 1.0f || __fadd_rn(xb, b.x) >= pf + 1.0f) continue;
+      }
       for (int iy = iy_lo; iy <= iy_hi; ++iy) {
         const float2 l = __ldg(&a.loc.table[((size_t)v * a.ny + iy) * a.loc.table_nx + ox]);
         const float x = __fadd_rn(xb, l.x);

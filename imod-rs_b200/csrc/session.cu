@@ -145,7 +145,7 @@ static void free_session(tg_session *s) {
   void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_volh, s->d_maxbits, s->d_mpart, s->d_pairs,
                   s->d_part, s->d_slice_stats, s->d_stats3, s->d_vg, s->d_vg2, s->d_weights,
                   s->d_conv, s->d_stretch, s->d_tw, s->d_err, s->d_lvinfo, s->d_lgoff, s->d_lxs,
-                  s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab, s->d_xtb};
+                  s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab, s->d_xtb, s->d_lbnd};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : s->ev)
@@ -159,7 +159,7 @@ void free_session_async(tg_session *s, cudaStream_t after) {
   void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_volh, s->d_maxbits, s->d_mpart, s->d_pairs,
                   s->d_part, s->d_slice_stats, s->d_stats3, s->d_vg, s->d_vg2, s->d_weights,
                   s->d_conv, s->d_stretch, s->d_tw, s->d_err, s->d_lvinfo, s->d_lgoff, s->d_lxs,
-                  s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab, s->d_xtb};
+                  s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab, s->d_xtb, s->d_lbnd};
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, after);
   for (auto &e : s->ev)
@@ -392,6 +392,7 @@ FpArgs fp_args(tg_session *s) {
   f.volh = s->d_volh;
   f.maxbits = s->d_maxbits;
   f.variant = s->fp_variant;
+  f.lbnd = s->d_lbnd;
   return f;
 }
 
@@ -681,6 +682,9 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
   }
   if (s->has_local && (rc = upload_local(s, g->local, g->local ? g->n_local : 0, vg2))) return fail(rc);
   // corrections per (view, slice, column): 8 bytes each, filled below
+  if (s->has_local && (rc = dalloc(s, &s->d_lbnd, (size_t)s->nviews * ((s->ny + LB_TILE - 1) / LB_TILE) *
+                                                      s->onx * sizeof(float2))))
+    return fail(rc);
   if (s->has_local && (rc = dalloc(s, &s->d_ltab, (size_t)s->nviews * s->ny * s->onx * sizeof(float2))))
     return fail(rc);
   if (dry) {
@@ -725,7 +729,10 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
     else cudaFree(s->d_stretch);
     s->d_stretch = nullptr;
   }
-  if (s->has_local) launch_local_table(local_dev(s), s->nviews, s->ny, s->onx, s->d_ltab, s->st);
+  if (s->has_local) {
+    launch_local_table(local_dev(s), s->nviews, s->ny, s->onx, s->d_ltab, s->st);
+    launch_local_bounds(s->d_ltab, s->nviews, s->ny, s->onx, s->d_lbnd, s->st);
+  }
   if ((ce = cudaStreamSynchronize(s->st)) != cudaSuccess) return fail(cuda_fail(ce, "sync"));
   *out = s;
   return TG_OK;

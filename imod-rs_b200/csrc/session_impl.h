@@ -45,6 +45,7 @@ struct tg_session {  // one tilt series resident on a device
   int *d_lgoff = nullptr;
   float *d_lxs = nullptr, *d_lys = nullptr, *d_lgdx = nullptr, *d_lgdy = nullptr;
   float2 *d_ltab = nullptr;  // local corrections per (view, slice, column)
+  float2 *d_lbnd = nullptr;  // their dx range per (view, slice tile, column): FpArgs::lbnd
   FftPlanDev plan{};
   bool use_conv = false;
   bool uploaded = false, prepared = false;

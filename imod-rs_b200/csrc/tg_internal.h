@@ -151,10 +151,16 @@ struct FpArgs {
   int variant;              // bit 0: 16 rows per thread (else 8); bit 1: interleaved copy;
                             // bit 2: 32 rows per thread in the half path (else 16);
                             // bit 3: FP32 reprojection also for half staging
+  // local alignment: per (view, tile t of LB_TILE slices, column) the min and max of the
+  // table's dx over slices [LB_TILE*(t-1), LB_TILE*(t+2)) (clipped to the series), or null
+  const float2 *lbnd;
 };
+constexpr int LB_TILE = 16;
 int launch_reproject(const FpArgs &a, cudaStream_t st);  // returns the kernels launched
 // fills L.table for every (view < nviews, slice < ny, column < onx)
 void launch_local_table(const LocalDev &L, int nviews, int ny, int onx, float2 *table, cudaStream_t st);
+// fills FpArgs::lbnd from the table: nviews * ceil(ny / LB_TILE) * onx entries
+void launch_local_bounds(const float2 *table, int nviews, int ny, int onx, float2 *bnd, cudaStream_t st);
 int fp_group_rows(int variant);
 int fp_half_rows(int variant);
 
