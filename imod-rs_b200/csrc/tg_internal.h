@@ -130,7 +130,7 @@ int bp_fast_row_align();  // slices per tile of the widest fast variant
 // floor(iy + dx*sin_xt) and the next, blended as the reference blends each
 // view's pair.  a.vol, a.mode (0, 1, 2), a.partial and the output constants as
 // in BpArgs; mode 0 writes XB_TILES partial-stat tiles per slice.
-constexpr int XB_TILES = 64;
+constexpr int XB_TILES = 16;  // depth tiles per slice (each block walks onz/16 depths)
 int launch_xt_blend(const BpArgs &a, const float *rows, float sin_xt, cudaStream_t st, int *ntiles_out);
 
 // ---- reprojection (main.rs:831-896) ----
