@@ -197,8 +197,7 @@ int tg_batch_synchronize(tg_batch *b) {
     TG_CUDA(cudaMemcpy(err, s->d_err, 16, cudaMemcpyDeviceToHost));
     if (err[0]) {
       cudaMemset(s->d_err, 0, 16);
-      set_error(err[0] & 1 ? "a bulk copy wait timed out" : "staging window outside the padded row");
-      return err[0] & 1 ? TG_ERR_TIMEOUT : TG_ERR_CUDA;
+      return device_error_status(err[0]);
     }
   }
   float ms = 0.f;

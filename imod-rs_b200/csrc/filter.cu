@@ -13,7 +13,9 @@
 
 #include <mutex>
 
+#include <algorithm>
 #include <cstdlib>
+#include <cstring>
 
 #include "tg_internal.h"
 
@@ -21,25 +23,48 @@ namespace tg {
 
 // ---------------------------------------------------------------------------
 // log10 (main.rs:608-613) fused with the per-view f64 sums (main.rs:616-623).
-// Grid (CH, nviews); every block owns a contiguous chunk of one view and
-// writes one f64 partial; a second kernel adds the CH partials in order, so
-// the result does not depend on scheduling.
+// The uploaded projections are read, never modified: with --log the log'd
+// values go to a second buffer, so every reconstruction repeats the whole
+// path.  Grid (CH, nviews); every block owns a contiguous chunk of one view
+// (16-byte loads and stores between a scalar head and tail) and writes one f64
+// partial; a second kernel adds the CH partials in order, so the result does
+// not depend on scheduling.  HBM-bound: 4 B read (+ 4 B written with --log)
+// per sample.
 // ---------------------------------------------------------------------------
 constexpr int MEAN_CH = 32;
 
-__global__ void __launch_bounds__(256) log_sum_kernel(float *raw, long npix, int do_log,
-                                                      double *partials) {
+// f32::max(0.001).log10(): computed in FP64 then rounded once
+__device__ __forceinline__ float log_sample(float x) { return (float)log10((double)fmaxf(x, 0.001f)); }
+
+template <bool LOG>
+__global__ void __launch_bounds__(256) log_sum_kernel(const float *__restrict__ raw, float *__restrict__ logd,
+                                                      long npix, double *partials) {
   const int v = blockIdx.y, c = blockIdx.x;
-  float *p = raw + (size_t)v * npix;
-  long c0 = npix * c / MEAN_CH, c1 = npix * (c + 1) / MEAN_CH;
+  const size_t base = (size_t)v * npix;
+  const long c0 = npix * c / MEAN_CH, c1 = npix * (c + 1) / MEAN_CH;
+  // [c0, a0): scalar head up to a 16-byte boundary; [a0, a1): float4; [a1, c1): tail
+  long a0 = c0 + (long)((4 - ((base + c0) & 3)) & 3);
+  if (a0 > c1) a0 = c1;
+  const long a1 = a0 + ((c1 - a0) & ~3L);
   double s = 0.0;
-  for (long i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-    float x = p[i];
-    if (do_log) {
-      // f32::max(0.001).log10(): computed in FP64 then rounded once
-      x = (float)log10((double)fmaxf(x, 0.001f));
-      p[i] = x;
+  for (long i = c0 + threadIdx.x; i < a0; i += blockDim.x) {
+    float x = raw[base + i];
+    if (LOG) logd[base + i] = x = log_sample(x);
+    s += (double)x;
+  }
+  const float4 *r4 = reinterpret_cast<const float4 *>(raw + base + a0);
+  float4 *l4 = LOG ? reinterpret_cast<float4 *>(logd + base + a0) : nullptr;
+  for (long i = threadIdx.x; i < (a1 - a0) / 4; i += blockDim.x) {
+    float4 x = __ldcs(r4 + i);
+    if (LOG) {
+      x = make_float4(log_sample(x.x), log_sample(x.y), log_sample(x.z), log_sample(x.w));
+      l4[i] = x;
     }
+    s += ((double)x.x + (double)x.y) + ((double)x.z + (double)x.w);
+  }
+  for (long i = a1 + threadIdx.x; i < c1; i += blockDim.x) {
+    float x = raw[base + i];
+    if (LOG) logd[base + i] = x = log_sample(x);
     s += (double)x;
   }
   __shared__ double red[8];
@@ -61,9 +86,10 @@ __global__ void means_final_kernel(const double *partials, long npix, int nviews
   means[v] = (float)(t / (double)npix);
 }
 
-void launch_log_means(float *raw, int npix, int nviews, int do_log, double *partials,
+void launch_log_means(const float *raw, float *logd, int npix, int nviews, double *partials,
                       float *means, cudaStream_t st) {
-  log_sum_kernel<<<dim3(MEAN_CH, nviews), 256, 0, st>>>(raw, npix, do_log, partials);
+  if (logd) log_sum_kernel<true><<<dim3(MEAN_CH, nviews), 256, 0, st>>>(raw, logd, npix, partials);
+  else log_sum_kernel<false><<<dim3(MEAN_CH, nviews), 256, 0, st>>>(raw, nullptr, npix, partials);
   means_final_kernel<<<(nviews + 127) / 128, 128, 0, st>>>(partials, npix, nviews, means);
 }
 
@@ -235,6 +261,18 @@ template <> struct Pack<TG_STORE_BF16> {
   }
 };
 
+// FP16 staging holds |v| < 65520 (larger values round to infinity).  Every packed
+// value's magnitude is tracked; a row that does not fit sets bit 2 of the
+// session's error word, which the host reports as TG_ERR_RANGE (a diverging SIRT
+// run whose residuals outgrow FP16; FP32 and BF16 staging have the f32 range).
+constexpr float FP16_LIMIT = 65520.0f;
+template <int STORE> __device__ __forceinline__ void range_track(float &mx, float v0, float v1) {
+  if (STORE == TG_STORE_FP16) mx = fmaxf(mx, fmaxf(fabsf(v0), fabsf(v1)));
+}
+template <int STORE> __device__ __forceinline__ void range_report(const FilterArgs &a, float mx) {
+  if (STORE == TG_STORE_FP16 && mx >= FP16_LIMIT && a.err) atomicOr(a.err, 4);
+}
+
 // Value pair (a, b) of element k of a final row, with the reference's fill
 // rule for samples whose left index is out of [0, nx-2] (main.rs:386-406).
 __device__ __forceinline__ void elem_ab(const float *row, int nx, int k, int fill_mode,
@@ -332,6 +370,7 @@ __global__ void __launch_bounds__(256) filter_kernel(FilterArgs a) {
     row1 = s1;
   }
   const float fillv = a.fill ? a.fill[v] : 0.0f;
+  float hmax = 0.0f;  // largest |value| packed into FP16 by this thread
   if (FMT == FMT_ROWS) {  // plain filtered rows written back over the input rows
     float *o0 = reinterpret_cast<float *>(a.out) + ((size_t)v * a.ny + r0) * n;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -353,8 +392,11 @@ __global__ void __launch_bounds__(256) filter_kernel(FilterArgs a) {
         reinterpret_cast<float4 *>(out)[e] = make_float4(a0, a1, b0, b1);
       } else {
         uint2 w;
+        const float d0 = __fsub_rn(b0, a0), d1 = __fsub_rn(b1, a1);
+        range_track<STORE>(hmax, a0, a1);
+        range_track<STORE>(hmax, d0, d1);
         w.x = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(a0, a1);
-        w.y = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(__fsub_rn(b0, a0), __fsub_rn(b1, a1));
+        w.y = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(d0, d1);
         reinterpret_cast<uint2 *>(out)[e] = w;
       }
     }
@@ -372,14 +414,16 @@ __global__ void __launch_bounds__(256) filter_kernel(FilterArgs a) {
         reinterpret_cast<float2 *>(o0)[e] = make_float2(a0, b0);
         if (has1) reinterpret_cast<float2 *>(o1)[e] = make_float2(a1, b1);
       } else {
-        reinterpret_cast<uint32_t *>(o0)[e] =
-            Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(a0, __fsub_rn(b0, a0));
+        const float d0 = __fsub_rn(b0, a0), d1 = __fsub_rn(b1, a1);
+        range_track<STORE>(hmax, a0, d0);
+        if (has1) range_track<STORE>(hmax, a1, d1);
+        reinterpret_cast<uint32_t *>(o0)[e] = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(a0, d0);
         if (has1)
-          reinterpret_cast<uint32_t *>(o1)[e] =
-              Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(a1, __fsub_rn(b1, a1));
+          reinterpret_cast<uint32_t *>(o1)[e] = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(a1, d1);
       }
     }
   }
+  range_report<STORE>(a, hmax);
 }
 
 // ---------------------------------------------------------------------------
@@ -552,6 +596,7 @@ __global__ void __launch_bounds__(N / V) filter_p2_kernel(FilterArgs a) {
   __syncthreads();
   // pack into the staging format with the reference's fill rule (main.rs:386-406)
   const float fillv = a.fill ? a.fill[v] : 0.0f;
+  float hmax = 0.0f;  // largest |value| packed into FP16 by this thread
   auto pair = [&](int k, float2 &lo, float2 &hi) {  // (row[k], row[k+1]) of both rows, or the fill
     if (k >= 0 && k + 1 < N) {
       lo = S[k];
@@ -575,8 +620,11 @@ __global__ void __launch_bounds__(N / V) filter_p2_kernel(FilterArgs a) {
         reinterpret_cast<float4 *>(out)[e] = make_float4(lo.x, lo.y, hi.x, hi.y);
       } else {
         uint2 w;
+        const float d0 = __fsub_rn(hi.x, lo.x), d1 = __fsub_rn(hi.y, lo.y);
+        range_track<STORE>(hmax, lo.x, lo.y);
+        range_track<STORE>(hmax, d0, d1);
         w.x = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.x, lo.y);
-        w.y = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(__fsub_rn(hi.x, lo.x), __fsub_rn(hi.y, lo.y));
+        w.y = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(d0, d1);
         reinterpret_cast<uint2 *>(out)[e] = w;
       }
     }
@@ -591,14 +639,16 @@ __global__ void __launch_bounds__(N / V) filter_p2_kernel(FilterArgs a) {
         reinterpret_cast<float2 *>(o0)[e] = make_float2(lo.x, hi.x);
         if (has1) reinterpret_cast<float2 *>(o1)[e] = make_float2(lo.y, hi.y);
       } else {
-        reinterpret_cast<uint32_t *>(o0)[e] =
-            Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.x, __fsub_rn(hi.x, lo.x));
+        const float d0 = __fsub_rn(hi.x, lo.x), d1 = __fsub_rn(hi.y, lo.y);
+        range_track<STORE>(hmax, lo.x, d0);
+        if (has1) range_track<STORE>(hmax, lo.y, d1);
+        reinterpret_cast<uint32_t *>(o0)[e] = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.x, d0);
         if (has1)
-          reinterpret_cast<uint32_t *>(o1)[e] =
-              Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.y, __fsub_rn(hi.y, lo.y));
+          reinterpret_cast<uint32_t *>(o1)[e] = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.y, d1);
       }
     }
   }
+  range_report<STORE>(a, hmax);
 }
 
 template <int N, int V, int FMT, int STORE> static void launch_p2(const FilterArgs &a, cudaStream_t st) {
@@ -665,9 +715,44 @@ constexpr int NOALLOC_MAX_NX = 8192;
 // layout: weights [n] | circulant kernel [n] | twiddles [2n]
 static __device__ __align__(256) float g_rw_scratch[4 * NOALLOC_MAX_NX];
 
+// The tables are computed on the host and travel to the array inside kernel
+// parameters (copied by value when each launch is issued), so no host buffer
+// has to outlive the call.  7680 floats = 30 KB per launch, under the 32 KB
+// kernel-parameter limit.
+constexpr int NOALLOC_CHUNK = 7680;
+struct NoallocChunk { float v[NOALLOC_CHUNK]; };
+__global__ void __launch_bounds__(256) noalloc_table_kernel(float *dst, int n, NoallocChunk c) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = c.v[i];
+}
+
 static std::mutex g_rw_mu;
-static float *g_rw_dev[128];                  // device address of g_rw_scratch per device ordinal
-static float g_rw_host[4 * NOALLOC_MAX_NX];   // host staging of the tables (static, no allocation)
+// device address of g_rw_scratch, per device ordinal, valid for the CUDA context
+// whose unique id is stored beside it (a reset device gets a new context)
+static float *g_rw_dev[128];
+static unsigned long long g_rw_ctx[128];
+static float g_rw_host[4 * NOALLOC_MAX_NX];   // host tables of the current call (under g_rw_mu)
+
+// Unique id of the calling thread's current CUDA context (0 if unavailable),
+// through the runtime's driver entry points (the library does not link libcuda).
+static unsigned long long current_context_id() {
+  typedef int (*CtxGetCurrent)(void **);
+  typedef int (*CtxGetId)(void *, unsigned long long *);
+  static CtxGetCurrent get_current = nullptr;
+  static CtxGetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, nullptr) == cudaSuccess)
+      get_current = reinterpret_cast<CtxGetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, nullptr) == cudaSuccess)
+      get_id = reinterpret_cast<CtxGetId>(f);
+  });
+  void *ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 }  // namespace tg
 
@@ -696,13 +781,15 @@ extern "C" int tg_apply_rweighting_device_noalloc(float *dev_proj, size_t in_nx,
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
   auto restore = [&]() { if (prev >= 0 && prev != device) cudaSetDevice(prev); };
-  if (!g_rw_dev[device]) {
-    // first call on this device: the array's device address (the host symbol
-    // is only a stand-in and must never be passed to a kernel)
+  const unsigned long long ctx = current_context_id();
+  if (!g_rw_dev[device] || ctx == 0 || ctx != g_rw_ctx[device]) {
+    // first call in this device's context: the array's device address (the host
+    // symbol is only a stand-in and must never be passed to a kernel)
     void *ptr = nullptr;
     e = cudaGetSymbolAddress(&ptr, g_rw_scratch);
     if (e != cudaSuccess) { restore(); return cuda_fail(e, "cudaGetSymbolAddress(g_rw_scratch)"); }
     g_rw_dev[device] = static_cast<float *>(ptr);
+    g_rw_ctx[device] = ctx;
   }
   const int n = (int)in_nx;
   float *hw = g_rw_host, *hconv = g_rw_host + NOALLOC_MAX_NX, *htw = g_rw_host + 2 * NOALLOC_MAX_NX;
@@ -722,14 +809,22 @@ extern "C" int tg_apply_rweighting_device_noalloc(float *dev_proj, size_t in_nx,
     }
   float *dev = g_rw_dev[device];
   cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
-  // pageable source: the copies have read the host tables when they return
-  if ((e = cudaMemcpyAsync(dev, hw, n * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (!radix && (e = cudaMemcpyAsync(dev + NOALLOC_MAX_NX, hconv, n * sizeof(float),
-                                      cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
-      (e = cudaMemcpyAsync(dev + 2 * NOALLOC_MAX_NX, htw, 2 * n * sizeof(float),
-                           cudaMemcpyHostToDevice, st)) != cudaSuccess) {
+  // tables -> the static array, in kernel-parameter chunks on the caller's stream
+  auto upload = [&](float *dst, const float *src, int count) -> cudaError_t {
+    static NoallocChunk chunk;  // under g_rw_mu; copied into each launch's parameters
+    for (int o = 0; o < count; o += NOALLOC_CHUNK) {
+      const int c = std::min(NOALLOC_CHUNK, count - o);
+      memcpy(chunk.v, src + o, (size_t)c * sizeof(float));
+      noalloc_table_kernel<<<1, 256, 0, st>>>(dst + o, c, chunk);
+      cudaError_t le = cudaGetLastError();
+      if (le != cudaSuccess) return le;
+    }
+    return cudaSuccess;
+  };
+  if ((e = upload(dev, hw, n)) != cudaSuccess || (!radix && (e = upload(dev + NOALLOC_MAX_NX, hconv, n)) != cudaSuccess) ||
+      (e = upload(dev + 2 * NOALLOC_MAX_NX, htw, 2 * n)) != cudaSuccess) {
     restore();
-    return cuda_fail(e, "cudaMemcpyAsync(noalloc tables)");
+    return cuda_fail(e, "noalloc table upload");
   }
   f.in = dev_proj;
   f.out = dev_proj;

@@ -207,10 +207,7 @@ void collect(tg_server *sv) {
       j->stats.amin = f[0];
       j->stats.amax = f[1];
       j->stats.amean = f[2];
-      if (err[0]) {
-        set_error(err[0] & 1 ? "a bulk copy wait timed out" : "staging window outside the padded row");
-        st = (err[0] & 1) ? TG_ERR_TIMEOUT : TG_ERR_CUDA;
-      }
+      if (err[0]) st = device_error_status(err[0]);
     }
     sv->active.erase(sv->active.begin() + i);
     end_job(sv, j, st);

@@ -31,6 +31,16 @@ int cuda_fail(cudaError_t e, const char *what) {
   set_error(std::string(what) + ": " + cudaGetErrorString(e));
   return e == cudaErrorMemoryAllocation ? TG_ERR_OOM : TG_ERR_CUDA;
 }
+int device_error_status(int word) {
+  if (word & 1) { set_error("a bounded device wait timed out"); return TG_ERR_TIMEOUT; }
+  if (word & 4) {
+    set_error("a filtered projection or SIRT residual exceeds the FP16 staging range (|v| >= 65520); "
+              "the SIRT run diverges or the data need FP32/BF16 staging");
+    return TG_ERR_RANGE;
+  }
+  set_error("staging window outside the padded row (internal error)");
+  return TG_ERR_CUDA;
+}
 
 static const float PI_F = 3.14159265358979323846f;  // std::f32::consts::PI
 
@@ -142,7 +152,7 @@ static void free_session(tg_session *s) {
   }
   if (s->st) cudaStreamSynchronize(s->st);
   if (s->sirt_exec) cudaGraphExecDestroy(s->sirt_exec);
-  void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_volh, s->d_maxbits, s->d_mpart, s->d_pairs,
+  void *ptrs[] = {s->d_raw, s->d_logd, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_volh, s->d_maxbits, s->d_mpart, s->d_pairs,
                   s->d_part, s->d_slice_stats, s->d_stats3, s->d_vg, s->d_vg2, s->d_weights,
                   s->d_conv, s->d_stretch, s->d_tw, s->d_err, s->d_lvinfo, s->d_lgoff, s->d_lxs,
                   s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab, s->d_xtb, s->d_lbnd};
@@ -156,7 +166,7 @@ static void free_session(tg_session *s) {
 
 void free_session_async(tg_session *s, cudaStream_t after) {
   if (s->sirt_exec) cudaGraphExecDestroy(s->sirt_exec);  // freed on completion if in flight
-  void *ptrs[] = {s->d_raw, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_volh, s->d_maxbits, s->d_mpart, s->d_pairs,
+  void *ptrs[] = {s->d_raw, s->d_logd, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_volh, s->d_maxbits, s->d_mpart, s->d_pairs,
                   s->d_part, s->d_slice_stats, s->d_stats3, s->d_vg, s->d_vg2, s->d_weights,
                   s->d_conv, s->d_stretch, s->d_tw, s->d_err, s->d_lvinfo, s->d_lgoff, s->d_lxs,
                   s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab, s->d_xtb, s->d_lbnd};
@@ -278,7 +288,7 @@ BpArgs bp_args(tg_session *s, int mode) {
 
 FilterArgs filter_args(tg_session *s, bool residual) {
   FilterArgs f{};
-  f.in = s->d_raw;
+  f.in = s->d_logd ? s->d_logd : s->d_raw;
   f.sub = residual ? s->d_sino : nullptr;
   f.out = s->d_pairs;
   f.weights = s->o.no_weight ? nullptr : s->d_weights;
@@ -298,6 +308,7 @@ FilterArgs filter_args(tg_session *s, bool residual) {
   f.store = s->store;
   f.inv_n = 1.0f / (float)s->nx;
   f.plan = s->plan;
+  f.err = s->d_err;
   return f;
 }
 
@@ -397,11 +408,10 @@ FpArgs fp_args(tg_session *s) {
 }
 
 int stage_front(tg_session *s, int *launches) {
-  if (!s->prepared) {
-    launch_log_means(s->d_raw, s->nx * s->ny, s->nz, s->o.log_transform, s->d_mpart, s->d_means, s->st);
-    *launches += 2;
-    s->prepared = true;
-  }
+  // every run starts from the uploaded projections: log10 into d_logd (--log) and the
+  // per-view means, as main.rs:608-623 does before each reconstruction
+  launch_log_means(s->d_raw, s->d_logd, s->nx * s->ny, s->nz, s->d_mpart, s->d_means, s->st);
+  *launches += 2;
   launch_filter(filter_args(s, false), s->st);
   *launches += 1;
   TG_CUDA(cudaGetLastError());
@@ -445,6 +455,7 @@ const char *tg_status_string(int st) {
     case TG_ERR_NOT_READY: return "not ready";
     case TG_ERR_NOT_FOUND: return "not found";
     case TG_ERR_CANCELLED: return "cancelled";
+    case TG_ERR_RANGE: return "value beyond the FP16 staging range";
     default: return "unknown status";
   }
 }
@@ -652,6 +663,7 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
       (rc = dalloc(s, &s->d_weights, (size_t)s->nx * 4)) || (rc = dalloc(s, &s->d_tw, (size_t)s->nx * 8)) ||
       (rc = dalloc(s, &s->d_stretch, (size_t)s->nviews * 4)) || (rc = dalloc(s, &s->d_err, 16)))
     return fail(rc);
+  if (opt->log_transform && (rc = dalloc(s, &s->d_logd, nproj * 4))) return fail(rc);
   if (!opt->gpu_compat && opt->sirt_iters > 0 && (rc = dalloc(s, &s->d_sino, nproj * 4))) return fail(rc);
   if (!opt->gpu_compat && opt->fake_sirt > 0 && (rc = dalloc(s, &s->d_tmp, nvol * 4))) return fail(rc);
   if (const char *e = getenv("TG_FP_VARIANT")) s->fp_variant = atoi(e) & 15;
@@ -748,7 +760,6 @@ int tg_upload_projections(tg_session *s, const float *host, size_t n) {
   TG_CUDA(cudaSetDevice(s->dev));
   TG_CUDA(cudaMemcpyAsync(s->d_raw, host, n * 4, cudaMemcpyHostToDevice, s->st));
   s->uploaded = true;
-  s->prepared = false;
   return TG_OK;
 }
 
@@ -758,7 +769,6 @@ int tg_set_projections_device(tg_session *s, const float *dev, size_t n) {
   TG_CUDA(cudaSetDevice(s->dev));
   TG_CUDA(cudaMemcpyAsync(s->d_raw, dev, n * 4, cudaMemcpyDeviceToDevice, s->st));
   s->uploaded = true;
-  s->prepared = false;
   return TG_OK;
 }
 
@@ -833,9 +843,7 @@ int tg_synchronize(tg_session *s) {
   TG_CUDA(cudaMemcpy(err, s->d_err, 16, cudaMemcpyDeviceToHost));
   if (err[0]) {
     cudaMemsetAsync(s->d_err, 0, 16, s->st);
-    if (err[0] & 1) { set_error("a bulk copy wait timed out"); return TG_ERR_TIMEOUT; }
-    set_error("staging window outside the padded row (internal error)");
-    return TG_ERR_CUDA;
+    return device_error_status(err[0]);
   }
   if (s->timed) {  // stage times of the last tg_reconstruct (not recorded for batched runs)
     float t[4] = {0, 0, 0, 0};

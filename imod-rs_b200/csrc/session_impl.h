@@ -31,7 +31,9 @@ struct tg_session {  // one tilt series resident on a device
   int padL = 0, PW = 0, rows_alloc = 0, variant = -1, ntiles_cap = 0;
   int dev = 0;
   cudaStream_t st = nullptr, own_st = nullptr;
-  float *d_raw = nullptr, *d_means = nullptr, *d_vol = nullptr, *d_sino = nullptr, *d_tmp = nullptr;
+  // d_raw: the projections as uploaded (never modified); d_logd: their log10 (--log),
+  // rewritten by every reconstruction so each run repeats the reference's whole path
+  float *d_raw = nullptr, *d_logd = nullptr, *d_means = nullptr, *d_vol = nullptr, *d_sino = nullptr, *d_tmp = nullptr;
   double *d_mpart = nullptr;
   void *d_pairs = nullptr;
   size_t pairs_bytes = 0;
@@ -48,7 +50,7 @@ struct tg_session {  // one tilt series resident on a device
   float2 *d_lbnd = nullptr;  // their dx range per (view, slice tile, column): FpArgs::lbnd
   FftPlanDev plan{};
   bool use_conv = false;
-  bool uploaded = false, prepared = false;
+  bool uploaded = false;
   bool timed = false;  // ev[] were recorded by the last tg_reconstruct
   size_t dev_bytes = 0;
   tg_run_info info{};
@@ -78,7 +80,7 @@ inline int fast_zf(const tg_session *s) { return s->xt_split ? 2 : s->zf_any ? 1
 int autotune(tg_session *s);
 // the tile variant already tuned for this shape (or pinned by TG_BP_VARIANT), else -1
 int tune_lookup(tg_session *s);
-// log10 + means on first use, then the filter stage of the WBP pass
+// log10 + per-view means, then the filter stage of the WBP pass
 int stage_front(tg_session *s, int *launches);
 // fake-SIRT passes, output transform (when the volume was stored raw) and statistics;
 // bp_ntiles: partial-stat tiles written by the back-projection in mode 0

@@ -35,7 +35,8 @@ struct StatPartial {
 };
 
 // ---- log transform + per-view means (main.rs:608-623) ----
-void launch_log_means(float *raw, int npix, int nviews, int do_log, double *partials,
+// logd == nullptr: means of raw; else logd = log10(max(raw, 0.001)) and its means
+void launch_log_means(const float *raw, float *logd, int npix, int nviews, double *partials,
                       float *means, cudaStream_t st);
 
 // ---- filter stage: R-weighting (main.rs:333-381), cosine stretch
@@ -62,6 +63,7 @@ struct FilterArgs {
   int fill_mode, cubic, fmt, store;
   float inv_n;
   FftPlanDev plan;
+  int *err;                 // session error word: bit 2 set when a value exceeds the FP16 range
 };
 void launch_filter(const FilterArgs &a, cudaStream_t st);
 // radial weight table of apps/tilt/src/main.rs:348-369 in f32 (host)
@@ -187,6 +189,10 @@ struct NvtxRange {
   NvtxRange &operator=(const NvtxRange &) = delete;
 };
 int cuda_fail(cudaError_t e, const char *what);
+// tg_status of a nonzero device error word (bit 0: a bounded wait gave up; bit 1:
+// staging window outside the padded row; bit 2: a value beyond the FP16 range),
+// with its message set
+int device_error_status(int word);
 #define TG_STR2(x) #x
 #define TG_STR(x) TG_STR2(x)
 #define TG_CUDA(call)                                                                       \

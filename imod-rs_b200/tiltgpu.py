@@ -21,7 +21,7 @@ TG_OK = 0
 STATUS = {0: "ok", -1: "invalid argument", -2: "out of device memory", -3: "CUDA error",
           -4: "device wait timed out", -5: "over memory budget", -6: "unsupported",
           -7: "no sm_100 CUDA device", -8: "input on which the reference panics",
-          -9: "not ready", -10: "not found", -11: "cancelled"}
+          -9: "not ready", -10: "not found", -11: "cancelled", -12: "value beyond the FP16 staging range"}
 FILL = {"mean": 0, "zero": 1, "edge": 2}
 STORAGE = {"fp32": 0, "fp16": 1, "bf16": 2}
 

@@ -38,7 +38,10 @@ typedef enum {
                                tilt angles than views with cosine stretch on) */
   TG_ERR_NOT_READY = -9,    /* tg_server_wait: job still running */
   TG_ERR_NOT_FOUND = -10,   /* unknown job id */
-  TG_ERR_CANCELLED = -11    /* job dropped by tg_server_destroy before admission */
+  TG_ERR_CANCELLED = -11,   /* job dropped by tg_server_destroy before admission */
+  TG_ERR_RANGE = -12        /* FP16 staging: a filtered projection or SIRT residual exceeds the
+                               FP16 range (|v| >= 65520), e.g. a diverging SIRT run; the
+                               volume is not valid.  FP32/BF16 staging never report it. */
 } tg_status;
 
 /* Fill modes of apps/tilt/src/main.rs:122-128 */
@@ -267,10 +270,14 @@ int tg_apply_rweighting(float *proj_data, size_t in_nx, size_t in_ny, size_t nz,
  * (a cudaStream_t as void*, NULL = legacy default stream).  Allocates nothing:
  * its weight/twiddle tables live in a static 128 KB device array, which limits
  * rows to in_nx <= 8192 (larger rows are rejected with TG_ERR_INVALID_ARG).
- * The first call on a device looks the array up (cudaGetSymbolAddress); make
- * that first call before any stream capture.  All calls on a device share the
- * array and it keeps the last call's tables: calls whose GPU work overlaps
- * race, so order them on one stream. */
+ * Each call writes its tables into the array with small kernels that carry
+ * them in their launch parameters, then filters with the generic mixed-radix
+ * kernel (for 2^k and 3*2^k rows the allocating paths use a faster
+ * register-resident FFT kernel; the results agree to rounding).  The first call
+ * in a device's context looks the array up (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  All calls on a device share the array
+ * and it keeps the last call's tables: calls whose GPU work overlaps race, so
+ * order them on one stream. */
 int tg_apply_rweighting_device_noalloc(float *dev_proj, size_t in_nx, size_t in_ny, size_t nz,
                                        float cutoff, float falloff, int32_t exact_filter_size,
                                        int32_t use_hamming, int32_t device, void *cuda_stream);
