@@ -138,6 +138,19 @@ def barrier(dist, world):
         dist.barrier()
 
 
+def hbm_peak():
+    """Measured HBM copy bandwidth of this pool's B200s (GB/s) and where it came from."""
+    for path in (os.path.join(ROOT, "MEASURED_PEAKS.json"), "/root/repo/MEASURED_PEAKS.json"):
+        try:
+            with open(path) as f:
+                v = json.load(f).get("hbm_gbs")
+            if v:
+                return float(v), "of measured (MEASURED_PEAKS.json hbm_gbs)"
+        except (OSError, ValueError, AttributeError):
+            pass
+    return 6650.0, "of fallback (6.65 TB/s, MEASURED_PEAKS.json absent)"
+
+
 def read_traffic():
     """Per-launch DRAM traffic of the back-projection kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "bp_fast_c2_fp16.md")
@@ -309,7 +322,10 @@ def run_ours(args):
                      "note": "shared-memory bytes of the back-projection kernel (4 B/update FP16 pair); "
                              "peak = 148 SMs x 128 B/clk x median SM clock sampled in the run"},
         "roofline_hbm": {"bound": "hbm", "achieved": (4.0 * nz * nx * ny + 4.0 * onx * onz * ny) / bp_s / 1e9,
-                         "peak": 6548.2, "unit": "GB/s", "note": "of measured (MEASURED_PEAKS.json)"},
+                         "peak": hbm_peak()[0], "unit": "GB/s",
+                         "note": "back-projection kernel: FP16 staged rows (4 B per sample: value and "
+                                 "difference) read + volume written; "
+                                 + hbm_peak()[1]},
         "e2e": {"value": e2e_upd / e2e_s, "unit": "updates/s", "h2d_bytes_per_step": n_proj * 4,
                 "d2h_bytes_per_step": int(np.prod(out_shape)) * 4 + 12},
         "gpu_launches": launches,
@@ -318,24 +334,33 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"], ref_rows = cpu_baseline(args, w, proj_d, nslices=acc_rows, want_rows=True)
         # error of both forms on those slices against the oracle's f32 restatement of the reference
+        # and against the oracle's FP64 data path with the reference's f32 geometry (ref64g),
+        # the bound of the FP16 form (rel-L2 <= 2e-3)
+        ref64 = oracle_rows64(w, proj_d, acc_rows)
         line["accuracy"] = {}
         for form, got in first.items():
-            d = got.astype(np.float64) - ref_rows.astype(np.float64)
-            line["accuracy"][form + "_vs_ref32"] = {
-                "rel_l2": float(np.linalg.norm(d) / np.linalg.norm(ref_rows.astype(np.float64))),
-                "max_abs": float(np.abs(d).max()), "ref_max_abs": float(np.abs(ref_rows).max()),
-                "slices": acc_rows}
+            for name, ref in (("ref32", ref_rows), ("ref64g", ref64)):
+                d = got.astype(np.float64) - ref.astype(np.float64)
+                line["accuracy"][f"{form}_vs_{name}"] = {
+                    "rel_l2": float(np.linalg.norm(d) / np.linalg.norm(ref.astype(np.float64))),
+                    "max_abs": float(np.abs(d).max()), "ref_max_abs": float(np.abs(ref).max()),
+                    "slices": acc_rows}
     if rank == 0 and world == 1 and args.workload == "c2" and not args.no_serving:
-        # the metric's latency half: a short served stream (full run: --workload serve)
+        # the metric's latency half and the north-star comparison: served FP16 against
+        # serial plain FP32, end to end (host copies included), on the same series
         del proj_d
         torch.cuda.empty_cache()
+        keys = ("workload", "jobs", "done", "failed", "latency_ms", "value", "device_busy_updates_per_s",
+                "serial_plain_fp32", "ratio_vs_serial_plain_fp32")
         try:
-            sv = serve_stream(20.0, args.serve_seconds, 0.05, 150.0, 16, n_large=1)
-            line["serving"] = {k: sv[k] for k in ("workload", "jobs", "done", "failed", "latency_ms", "value",
-                                                  "device_busy_updates_per_s", "serial_plain_fp32")}
-            line["serving"]["unit"] = "updates/s"
+            sv, pool = serve_stream(20.0, args.serve_seconds, 0.05, 150.0, 16, n_large=1)
+            line["serving"] = {k: sv[k] for k in keys} | {"unit": "updates/s"}
+            sat, _ = serve_stream(40.0, args.saturated_seconds, 0.05, 150.0, 16, n_large=1, pool=pool, seed=21)
+            line["serving_saturated"] = {k: sat[k] for k in keys} | {"unit": "updates/s"}
+            del pool
+            line["c4_end_to_end"] = c4_at_once()
         except Exception as exc:  # the throughput line above stands on its own
-            line["serving"] = {"error": repr(exc)[:200]}
+            line["serving_error"] = repr(exc)[:200]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -365,6 +390,18 @@ def cpu_baseline(args, w, proj_d=None, nslices=16, want_rows=False):
     return (res, rows) if want_rows else res
 
 
+def oracle_rows64(w, proj_d, nslices):
+    """ref64g (FP64 data path, the reference's f32 sampling geometry) of slices [0, nslices)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    nx, ny, onx, onz, ang = w["nx"], w["ny"], w["onx"], w["onz"], w["angles"]
+    nz = len(ang)
+    proj = proj_d.cpu().numpy().reshape(nz, ny, nx)
+    p = O.Params(nx, ny, nz, ang, width=onx, thickness=onz, radial=w["radial"], log=True)
+    return O.wbp_rows(p, proj, 0, nslices, nthreads=os.cpu_count() or 1, precision="64g")
+
+
 def seeded_rows(nz, ny, nx, nrows, seed=5):
     """Seeded Poisson-like counts for the rows a bounded CPU sample reads (timing is data-independent)."""
     rng = np.random.default_rng(seed)
@@ -385,10 +422,12 @@ def run_reference(args):
     w = c2_workload()
     nx, ny, onx, onz, ang = w["nx"], w["ny"], w["onx"], w["onz"], w["angles"]
     nz = len(ang)
-    nsl = 8
+    cores = os.cpu_count() or 1
+    # the oracle parallelises over slices (as the reference's rayon loop over Y does):
+    # two slices per host thread keep every core busy
+    nsl = max(8, 2 * cores)
     proj = seeded_rows(nz, ny, nx, nsl)
     p = O.Params(nx, ny, nz, ang, width=onx, thickness=onz, radial=w["radial"], log=True)
-    cores = os.cpu_count() or 1
     for _ in range(args.warmup):
         O.wbp_rows(p, proj, 0, nsl, nthreads=cores)
     t0 = time.perf_counter()
@@ -578,56 +617,48 @@ def run_c4(args):
     print(json.dumps(line), flush=True)
 
 
-def serve_stream(rate, duration, large_frac, budget_gb, pool_small, n_large=2):
-    """Poisson request stream through tg_server (continuous batching, HBM admission
-    budget) with p50/p99 latency; beside it the same arrivals served one at a time
-    by plain FP32 sessions (each pool series timed once end to end, the arrivals
-    replayed through one first-in first-out server with those service times)."""
-    import torch
-
-    import tiltgpu as T
-    rng = np.random.default_rng(20)
-    small = c4_jobs(pool_small, seed=5)
-    big_ang = np.arange(-60, 61, 1.0).astype(np.float32)
-    large = [dict(w=2048, nv=121, ang=big_ang, thick=800, sirt=0, seed=9000 + k, noise=0.5)
-             for k in range(n_large)]
+def make_pool(T, torch, jobs):
+    """Seeded projections of each job in pinned host memory, every shape tuned in both
+    forms (FP16 staging, plain FP32) outside any timed region."""
     t0 = time.perf_counter()
-    pool = [(j, synth_job(T, torch, j)) for j in small + large]
+    pool = [(j, synth_job(T, torch, j)) for j in jobs]
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
-    print(f"# pool of {len(pool)} seeded series ready in {time.perf_counter() - t0:.1f}s", file=sys.stderr,
-          flush=True)
-    arrivals, t = [], 0.0
-    while True:
-        t += rng.exponential(1.0 / rate)
-        if t >= duration:
-            break
-        if rng.random() < large_frac:
-            k = len(small) + int(rng.integers(0, len(large)))
-        else:
-            k = int(rng.integers(0, len(small)))
-        arrivals.append((t, k))
-    # pinned output rings: every result is copied out; contents are not checked here
-    max_small = max(j["w"] * j["w"] * j["thick"] for j in small)
-    ring_small = [torch.empty(max_small, dtype=torch.float32, pin_memory=True) for _ in range(4)]
-    ring_large = torch.empty(2048 * 2048 * 800, dtype=torch.float32, pin_memory=True)
-
-    def out_for(i, j):
-        n = j["w"] * j["w"] * j["thick"]
-        buf = ring_large if j["w"] == 2048 else ring_small[i % len(ring_small)]
-        return buf[:n].numpy().reshape(j["w"], j["thick"], j["w"])
-
-    def kw_of(j, storage, sirt=None):
-        return dict(thickness=j["thick"], sirt=j["sirt"] if sirt is None else sirt, radial=(0.35, 0.035),
-                    storage=storage)
-
-    # tune the tile shape of every pool shape (both forms) outside the timed stream
     for j, h in pool:
         for storage in ("fp16", "fp32"):
-            with T.Session(j["w"], j["w"], len(j["ang"]), j["ang"], **kw_of(j, storage, sirt=0)) as s:
+            with T.Session(j["w"], j["w"], len(j["ang"]), j["ang"], **job_kw(j, storage, sirt=0)) as s:
                 s.upload(h.numpy())
                 s.reconstruct()
     torch.cuda.empty_cache()
+    print(f"# pool of {len(pool)} seeded series ready in {time.perf_counter() - t0:.1f}s", file=sys.stderr,
+          flush=True)
+    return pool
+
+
+def job_kw(j, storage, sirt=None):
+    return dict(thickness=j["thick"], sirt=j["sirt"] if sirt is None else sirt, radial=(0.35, 0.035),
+                storage=storage)
+
+
+class OutRings:
+    """Pinned host output buffers: every result is copied out in full; contents are not
+    checked here (jobs that share a ring slot overwrite each other's bytes)."""
+
+    def __init__(self, torch, pool, n=4):
+        small = [j["w"] * j["w"] * j["thick"] for j, _ in pool if j["w"] < 2048]
+        large = [j["w"] * j["w"] * j["thick"] for j, _ in pool if j["w"] >= 2048]
+        self.small = [torch.empty(max(small or [1]), dtype=torch.float32, pin_memory=True) for _ in range(n)]
+        self.large = torch.empty(max(large), dtype=torch.float32, pin_memory=True) if large else None
+
+    def out(self, i, j):
+        n = j["w"] * j["w"] * j["thick"]
+        buf = self.large if j["w"] >= 2048 else self.small[i % len(self.small)]
+        return buf[:n].numpy().reshape(j["w"], j["thick"], j["w"])
+
+
+def served_run(T, pool, arrivals, budget_gb, rings):
+    """Submit pool[k] at each arrival time (seconds from the start) to one tg_server
+    (FP16 staging, continuous batching, HBM admission budget); wait for all."""
     sampler = ClockSampler(0)
     sv = T.Server(device=0, budget_bytes=int(budget_gb * 1e9), max_active=64)
     ids = []
@@ -638,38 +669,18 @@ def serve_stream(rate, duration, large_frac, budget_gb, pool_small, n_large=2):
         if ta > now:
             time.sleep(ta - now)
         j, h = pool[k]
-        ids.append(sv.submit(h.numpy(), j["ang"], out=out_for(i, j), tag=k, **kw_of(j, "fp16")))
+        ids.append(sv.submit(h.numpy(), j["ang"], out=rings.out(i, j), tag=k, **job_kw(j, "fp16")))
     results = [sv.wait(jid) for jid in ids]
     wall = time.perf_counter() - start
     clocks = sampler.stop()
     info = sv.info()
     sv.close()
     done = [r for r in results if r["state"] == "done"]
-    lat = np.array([r["done_ms"] - r["submit_ms"] for r in done])
-    span_ms = max(r["done_ms"] for r in done) - min(r["submit_ms"] for r in done)
+    lat = np.array([r["done_ms"] - r["submit_ms"] for r in done]) if done else np.zeros(1)
+    span_ms = (max(r["done_ms"] for r in done) - min(r["submit_ms"] for r in done)) if done else 1.0
     upd = sum(r["updates"] for r in done)
-    service = []
-    for i, (j, h) in enumerate(pool):
-        out = out_for(i, j)
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        with T.Session(j["w"], j["w"], len(j["ang"]), j["ang"], **kw_of(j, "fp32")) as s:
-            s.upload(h.numpy())
-            s.reconstruct()
-            s.download(out=out)
-        service.append(time.perf_counter() - t1)
-    free_at, serial_lat = 0.0, []
-    for ta, k in arrivals:
-        begin = max(ta, free_at)
-        free_at = begin + service[k]
-        serial_lat.append(free_at - ta)
-    arr_upd = sum(job_updates(pool[k][0]) for _, k in arrivals)
-    serial_busy = sum(service[k] for _, k in arrivals)
-    line = {"metric": METRIC, "value": upd / (span_ms / 1e3), "unit": "updates/s", "n_gpus": 1,
-            "workload": (f"serve: Poisson {rate} jobs/s for {duration:.0f} s, C4 sizes "
-                         f"({len(small)} seeded series) + {large_frac:.0%} 2048^2x121-view WBP jobs "
-                         f"(thickness 800), FP16 staging, budget {budget_gb:.0f} GB"),
-            "jobs": len(arrivals), "done": len(done), "failed": len(results) - len(done),
+    return {"value": upd / (span_ms / 1e3), "jobs": len(arrivals), "done": len(done),
+            "failed": len(results) - len(done),
             "failures": sorted({f'{r["status"]}: {r["message"]}' for r in results if r["state"] != "done"})[:5],
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "max": float(lat.max())},
@@ -677,22 +688,103 @@ def serve_stream(rate, duration, large_frac, budget_gb, pool_small, n_large=2):
             "gpu_round_s": info["gpu_round_ms"] / 1e3, "host_round_s": info["host_round_ms"] / 1e3,
             "host_admit_s": info["host_admit_ms"] / 1e3, "oom_requeues": info["oom_requeues"],
             "bytes_peak": info["bytes_peak"],
-            "device_busy_updates_per_s": upd / max(info["gpu_round_ms"] / 1e3, 1e-9),
-            "serial_plain_fp32": {"value": arr_upd / serial_busy, "unit": "updates/s",
-                                  "utilisation": serial_busy / duration,
-                                  "latency_ms_fifo_replay": {
-                                      "p50": float(np.percentile(serial_lat, 50)) * 1e3,
-                                      "p99": float(np.percentile(serial_lat, 99)) * 1e3},
-                                  "how": "each pool series timed once end to end (upload, reconstruct, "
-                                         "download); the arrivals replayed through one FIFO server"},
-            "clocks": clocks, "data": "synthetic seeded phantoms, projections from pinned host memory"}
-    return line
+            "device_busy_updates_per_s": upd / max(info["gpu_round_ms"] / 1e3, 1e-9), "clocks": clocks}
+
+
+def serial_service_times(T, torch, pool, rings):
+    """Plain FP32, one series at a time, end to end: upload from pinned memory,
+    reconstruct, download the whole volume (seconds per pool series)."""
+    service = []
+    for i, (j, h) in enumerate(pool):
+        out = rings.out(i, j)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        with T.Session(j["w"], j["w"], len(j["ang"]), j["ang"], **job_kw(j, "fp32")) as s:
+            s.upload(h.numpy())
+            s.reconstruct()
+            s.download(out=out)
+        service.append(time.perf_counter() - t1)
+    return service
+
+
+def serve_stream(rate, duration, large_frac, budget_gb, pool_small, n_large=2, pool=None, seed=20):
+    """Poisson request stream through tg_server (continuous batching, HBM admission
+    budget) with p50/p99 latency; beside it the same arrivals served one at a time
+    by plain FP32 sessions (each pool series timed once end to end, the arrivals
+    replayed through one first-in first-out server with those service times)."""
+    import torch
+
+    import tiltgpu as T
+    rng = np.random.default_rng(seed)
+    if pool is None:
+        small = c4_jobs(pool_small, seed=5)
+        big_ang = np.arange(-60, 61, 1.0).astype(np.float32)
+        large = [dict(w=2048, nv=121, ang=big_ang, thick=800, sirt=0, seed=9000 + k, noise=0.5)
+                 for k in range(n_large)]
+        pool = make_pool(T, torch, small + large)
+    small_idx = [k for k, (j, _) in enumerate(pool) if j["w"] < 2048]
+    large_idx = [k for k, (j, _) in enumerate(pool) if j["w"] >= 2048]
+    arrivals, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
+            break
+        if large_idx and rng.random() < large_frac:
+            k = large_idx[int(rng.integers(0, len(large_idx)))]
+        else:
+            k = small_idx[int(rng.integers(0, len(small_idx)))]
+        arrivals.append((t, k))
+    rings = OutRings(torch, pool)
+    sv = served_run(T, pool, arrivals, budget_gb, rings)
+    service = serial_service_times(T, torch, pool, rings)
+    free_at, serial_lat = 0.0, []
+    for ta, k in arrivals:
+        begin = max(ta, free_at)
+        free_at = begin + service[k]
+        serial_lat.append(free_at - ta)
+    arr_upd = sum(job_updates(pool[k][0]) for _, k in arrivals)
+    serial_busy = sum(service[k] for _, k in arrivals)
+    serial = {"value": arr_upd / serial_busy, "unit": "updates/s", "utilisation": serial_busy / duration,
+              "latency_ms_fifo_replay": {"p50": float(np.percentile(serial_lat, 50)) * 1e3,
+                                         "p99": float(np.percentile(serial_lat, 99)) * 1e3},
+              "how": "each pool series timed once end to end (upload, reconstruct, download); "
+                     "the arrivals replayed through one FIFO server"}
+    n_small = len(small_idx)
+    line = {"metric": METRIC, "unit": "updates/s", "n_gpus": 1,
+            "workload": (f"serve: Poisson {rate} jobs/s for {duration:.0f} s, C4 sizes "
+                         f"({n_small} seeded series) + {large_frac:.0%} 2048^2x121-view WBP jobs "
+                         f"(thickness 800), FP16 staging, budget {budget_gb:.0f} GB"),
+            **sv, "serial_plain_fp32": serial, "ratio_vs_serial_plain_fp32": sv["value"] / serial["value"],
+            "data": "synthetic seeded phantoms, projections from pinned host memory"}
+    return line, pool
+
+
+def c4_at_once(budget_gb=150.0, pool=None):
+    """The 64 uneven C4 series (WBP:SIRT(10) 3:1) submitted together to the server
+    (FP16 staging, continuous batching, every projection copied in from pinned host
+    memory and every volume copied out) against plain FP32 series run one after
+    another end to end (upload, reconstruct, download)."""
+    import torch
+
+    import tiltgpu as T
+    if pool is None:
+        pool = make_pool(T, torch, c4_jobs())
+    rings = OutRings(torch, pool)
+    sv = served_run(T, pool, [(0.0, k) for k in range(len(pool))], budget_gb, rings)
+    service = serial_service_times(T, torch, pool, rings)
+    upd = sum(job_updates(j) for j, _ in pool)
+    plain = upd / sum(service)
+    return {"workload": "c4: 64 uneven series (widths 256-1024, 41-121 views, thickness 100-500, "
+                        "WBP:SIRT(10) 3:1), all submitted at once, host copies included",
+            "batched_fp16_served": sv["value"], "plain_fp32_serial": plain,
+            "ratio_vs_plain_fp32": sv["value"] / plain, "done": sv["done"], "failed": sv["failed"],
+            "wall_s": sv["wall_s"], "serial_s": sum(service), "unit": "updates/s"}
 
 
 def run_serve(args):
     import torch
     torch.cuda.set_device(0)
-    line = serve_stream(args.rate, args.duration, args.large_frac, args.budget_gb, args.pool)
+    line, _ = serve_stream(args.rate, args.duration, args.large_frac, args.budget_gb, args.pool)
     print(json.dumps(line), flush=True)
 
 
@@ -714,7 +806,9 @@ def main():
     ap.add_argument("--pool", type=int, default=32, help="serve: distinct seeded C4-size series")
     ap.add_argument("--serve-seconds", type=float, default=10.0,
                     help="default run: seconds of the short served stream reported under 'serving'")
-    ap.add_argument("--no-serving", action="store_true", help="default run: skip the short served stream")
+    ap.add_argument("--saturated-seconds", type=float, default=15.0,
+                    help="default run: seconds of the saturated (40 jobs/s) served stream")
+    ap.add_argument("--no-serving", action="store_true", help="default run: skip the served streams and C4")
     ap.add_argument("--forms", default=None, help="staging precisions to time (c1/c2: fp32,fp16; c3: fp32,bf16)")
     ap.add_argument("--profile", action="store_true",
                     help="time the requested forms only (no e2e, no CPU baseline); for ncu captures")

@@ -86,6 +86,7 @@ def lib():
             "or_forward_project64g": (i, [P, P, P]),
             "or_output_stats32": (None, [P, i, i, i, f, f, f, P]),
             "or_wbp_rows32": (i, [P, P, P, i, i, i]),
+            "or_wbp_rows64g": (i, [P, P, P, i, i, i]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(_lib, name)
@@ -262,13 +263,18 @@ def output_stats(vol: np.ndarray, densweight=1.0, outscale=1.0, outadd=0.0):
     return v, {"amin": st.amin, "amax": st.amax, "amean": st.amean}
 
 
-def wbp_rows(params: Params, proj: np.ndarray, y0: int, y1: int, nthreads=0):
-    """Timed CPU baseline: the reference's WBP flow for slices [y0, y1)."""
+def wbp_rows(params: Params, proj: np.ndarray, y0: int, y1: int, nthreads=0, precision=32):
+    """The reference's WBP flow for slices [y0, y1) (means over whole views).
+
+    precision 32: ref32, the timed CPU baseline; "64g": FP64 data path with the
+    reference's f32 sampling geometry (error checks of the half-staging forms)."""
     nthreads = nthreads or os.cpu_count() or 1
     p = np.ascontiguousarray(proj, dtype=np.float32)
-    vol = np.zeros((y1 - y0, params.out_nz, params.out_nx), np.float32)
+    dt = np.float32 if precision == 32 else np.float64
+    vol = np.zeros((y1 - y0, params.out_nz, params.out_nx), dt)
     s = params.struct()
-    rc = lib().or_wbp_rows32(C.byref(s), _ptr(p), _ptr(vol), y0, y1, nthreads)
+    fn = lib().or_wbp_rows32 if precision == 32 else lib().or_wbp_rows64g
+    rc = fn(C.byref(s), _ptr(p), _ptr(vol), y0, y1, nthreads)
     if rc != 0:
         raise RuntimeError(f"oracle wbp_rows failed with code {rc}")
     return vol

@@ -677,44 +677,56 @@ void or_output_stats32(float *vol, int a, int b, int c, float dw, float os, floa
   output_stats<float>(vol, a, b, c, dw, os, oa, st);
 }
 
-// Timed CPU baseline: the reference's WBP flow restricted to slices [y0,y1).
-// Only the projection rows those slices read are filtered (all rows of the
-// band when x-tilt or local alignment bends the rays).
-int or_wbp_rows32(const or_params *p, const float *proj_in, float *vol_rows, int y0, int y1, int nt) {
+}  // extern "C"
+
+namespace {
+// The reference's WBP flow (main.rs:607-653, 1002-1090) restricted to slices
+// [y0, y1): only the projection rows those slices read are log'd, filtered and
+// stretched (all rows when x-tilt or local alignment bends the rays); the
+// per-view means still cover the whole view.  G = sampling geometry type,
+// T = data type, as in run().
+template <typename G, typename T>
+int wbp_rows(const or_params *p, const float *proj_in, T *vol_rows, int y0, int y1, int nt) {
   const int nx = p->nx, ny = p->ny, nz = p->nz;
   int halo = 0;
   if (p->xtilt || p->has_local) halo = ny;  // conservative: whole stack
-  int r0 = std::max(0, y0 - halo), r1 = std::min(ny, y1 + halo);
-  std::vector<float> proj((size_t)nx * ny * nz, 0.0f);
+  const int r0 = std::max(0, y0 - halo), r1 = std::min(ny, y1 + halo);
+  std::vector<T> proj((size_t)nx * ny * nz, (T)0);
+  auto logv = [&](float x) -> T { return p->log_transform ? K<T>::log10_(std::fmax((T)x, (T)0.001f)) : (T)x; };
   for (int v = 0; v < nz; ++v)
-    std::memcpy(&proj[((size_t)v * ny + r0) * nx], proj_in + ((size_t)v * ny + r0) * nx,
-                sizeof(float) * (size_t)(r1 - r0) * nx);
-  std::vector<float> means(nz);
-  if (p->log_transform)
-    for (int v = 0; v < nz; ++v)
-      for (size_t i = ((size_t)v * ny + r0) * nx; i < ((size_t)v * ny + r1) * nx; ++i)
-        proj[i] = log10f(std::fmax(proj[i], 0.001f));
-  for (int v = 0; v < nz; ++v) {  // means need the whole view (input is the full stack)
+    for (size_t i = ((size_t)v * ny + r0) * nx; i < ((size_t)v * ny + r1) * nx; ++i) proj[i] = logv(proj_in[i]);
+  std::vector<T> means(nz);
+  parallel_for(nz, nt, [&](int v) {  // main.rs:616-623 over the whole view
     double s = 0.0;
     const float *d = proj_in + (size_t)v * nx * ny;
-    for (size_t i = 0; i < (size_t)nx * ny; ++i) s += (double)(p->log_transform ? log10f(std::fmax(d[i], 0.001f)) : d[i]);
-    means[v] = (float)(s / (double)((size_t)nx * ny));
-  }
-  std::vector<float> rows;  // gather the band rows contiguously for the FFT
-  rows.resize((size_t)nz * (r1 - r0) * nx);
+    for (size_t i = 0; i < (size_t)nx * ny; ++i) s += (double)logv(d[i]);
+    means[v] = (T)(s / (double)((size_t)nx * ny));
+  });
+  std::vector<T> rows((size_t)nz * (r1 - r0) * nx);  // the band rows, contiguous for the FFT
   for (int v = 0; v < nz; ++v)
-    std::memcpy(&rows[(size_t)v * (r1 - r0) * nx], &proj[((size_t)v * ny + r0) * nx], sizeof(float) * (size_t)(r1 - r0) * nx);
+    std::memcpy(&rows[(size_t)v * (r1 - r0) * nx], &proj[((size_t)v * ny + r0) * nx], sizeof(T) * (size_t)(r1 - r0) * nx);
   if (!p->no_weight)
-    rweight<float>(rows.data(), nx, nz * (r1 - r0), p->cutoff, p->falloff, p->exact_filter_size, p->hamming, nt);
+    rweight<T>(rows.data(), nx, nz * (r1 - r0), (T)p->cutoff, (T)p->falloff, p->exact_filter_size, p->hamming, nt);
   for (int v = 0; v < nz; ++v)
-    std::memcpy(&proj[((size_t)v * ny + r0) * nx], &rows[(size_t)v * (r1 - r0) * nx], sizeof(float) * (size_t)(r1 - r0) * nx);
+    std::memcpy(&proj[((size_t)v * ny + r0) * nx], &rows[(size_t)v * (r1 - r0) * nx], sizeof(T) * (size_t)(r1 - r0) * nx);
   if (!p->no_cosine_stretch) {
-    int rc = cosine_stretch<float, float>(proj.data(), nx, ny, nz, p->angles, p->n_angles, p->cosine_cubic,
-                                          p->max_cosine_tilt, r0, r1);
+    int rc = cosine_stretch<G, T>(proj.data(), nx, ny, nz, p->angles, p->n_angles, p->cosine_cubic,
+                                  (G)p->max_cosine_tilt, r0, r1);
     if (rc) return rc;
   }
-  backproject<float, float>(p, proj.data(), means.data(), vol_rows, y0, y1, nt);
+  backproject<G, T>(p, proj.data(), means.data(), vol_rows, y0, y1, nt);
   return 0;
+}
+}  // namespace
+
+extern "C" {
+// Timed CPU baseline (f32, the reference's arithmetic) and its FP64 form with the
+// reference's f32 sampling geometry (ref64g) for error checks on slice subsets.
+int or_wbp_rows32(const or_params *p, const float *proj_in, float *vol_rows, int y0, int y1, int nt) {
+  return wbp_rows<float, float>(p, proj_in, vol_rows, y0, y1, nt);
+}
+int or_wbp_rows64g(const or_params *p, const float *proj_in, double *vol_rows, int y0, int y1, int nt) {
+  return wbp_rows<float, double>(p, proj_in, vol_rows, y0, y1, nt);
 }
 
 }  // extern "C"

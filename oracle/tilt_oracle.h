@@ -111,6 +111,8 @@ void or_output_stats32(float *vol, int out_nx, int out_nz, int out_ny, float den
  * rows [y0,y1) of every view then backprojection of those slices. */
 int or_wbp_rows32(const or_params *p, const float *proj, float *vol_rows, int y0, int y1,
                   int nthreads);
+int or_wbp_rows64g(const or_params *p, const float *proj, double *vol_rows, int y0, int y1,
+                   int nthreads);
 
 #ifdef __cplusplus
 }

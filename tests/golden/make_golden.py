@@ -1,7 +1,8 @@
 """Extract the boundary test vectors of the reference's own unit tests.
 
 Reads crates/imod-mrc/src/tests.rs and crates/imod-transforms/src/tests.rs of
-the imod-rs source tree (path given as argv[1], default /root/reference) and
+the imod-rs source tree (its root is given as argv[1], or in the environment
+variable IMOD_RS_SRC) and
 writes tests/golden/reference_vectors.json: for each reference test the
 constructor arguments, labels, statistics and the data-generating expression,
 with the file:line it came from.  Every expected pattern is asserted, so a
@@ -14,7 +15,7 @@ import os
 import re
 import sys
 
-SRC = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+SRC = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("IMOD_RS_SRC", "")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_vectors.json")
 
 
@@ -37,6 +38,8 @@ def one(pattern, s, conv=str):
 
 
 def main():
+    if not SRC or not os.path.isdir(SRC):
+        sys.exit("usage: make_golden.py <imod-rs source root>  (or set IMOD_RS_SRC)")
     mrc_path = os.path.join(SRC, "crates/imod-mrc/src/tests.rs")
     tlt_path = os.path.join(SRC, "crates/imod-transforms/src/tests.rs")
     mrc = open(mrc_path).read()

@@ -41,3 +41,10 @@ def test_c4_jobs_are_seeded_and_in_range():
         assert np.all(np.diff(j["ang"]) > 0) and 49.0 < -j["ang"][0] < 71.0
     j = a[0]
     assert bench.job_updates(j) == float(j["w"]) ** 2 * j["thick"] * len(j["ang"]) * (1 + 2 * j["sirt"])
+
+
+def test_hbm_peak_is_read_from_the_measured_file(tmp_path, monkeypatch):
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"hbm_gbs": 6463.0}))
+    v, how = bench.hbm_peak()
+    assert v == 6463.0 and "measured" in how

@@ -369,9 +369,9 @@ def test_synthetic_phantom_is_seeded():
     assert np.isfinite(a).all()
 
 
-def test_c1_size_subset_and_half_error():
+def test_c1_size_subset_and_linearity():
     # config-1 geometry (61 views, 512^2 -> 512x512x200): the oracle checks a
-    # subset of slices; FP16 is checked against FP32 on the whole volume
+    # subset of slices (FP16 against the FP64 oracle: test_gpu_parity_configs.py)
     ang = angles(-60, 60, 2)
     nx = ny = 512
     proj = T.synth_projections(ang, nx=nx, ny=ny, vol_nz=200, n_ell=300, rmin=3, rmax=40,
@@ -379,13 +379,11 @@ def test_c1_size_subset_and_half_error():
                                noise_kind=1, noise=0.5, seed=1)
     kw = dict(radial=(0.35, 0.035), thickness=200)
     v32, s32 = T.reconstruct(proj, ang, storage="fp32", **kw)
-    v16, _ = T.reconstruct(proj, ang, storage="fp16", **kw)
     p = O.Params(nx, ny, len(ang), ang, **kw)
     ys = (0, 8)
     ref = O.wbp_rows(p, proj, *ys)
     out, _ = O.output_stats(ref)
     assert rel_l2(v32[ys[0]:ys[1]], out) <= TOL_FP32
-    assert rel_l2(v16, v32) <= TOL_HALF
     # linearity of the whole path in the projections (size-independent property)
     v2, _ = T.reconstruct((2.0 * proj).astype(np.float32), ang, storage="fp32", **kw)
     assert rel_l2(v2, 2.0 * v32) <= 1e-6

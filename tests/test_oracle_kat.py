@@ -195,3 +195,16 @@ def test_linear_stretch_formula():
         else:
             want = 0.0
         assert abs(out[ox] - want) <= 2e-7 * max(1.0, abs(want))
+
+
+@pytest.mark.parametrize("precision", [32, "64g"])
+def test_wbp_rows_equals_whole_run_slices(precision):
+    # the row-subset flow (means over whole views, only the band rows filtered) gives
+    # the same slices as the whole-volume run, in both the f32 and the FP64 forms
+    nz, ny, nx = 9, 12, 48
+    proj = (smooth_stack(nz, ny, nx, seed=9) * 100.0 + 1000.0).astype(np.float32)
+    ang = angles(-48, 48, 12)
+    p = O.Params(nx, ny, nz, ang, thickness=20, radial=(0.35, 0.035), log=True)
+    whole, _ = O.run(p, proj, precision)
+    rows = O.wbp_rows(p, proj, 3, 8, nthreads=4, precision=precision)
+    np.testing.assert_array_equal(rows, whole[3:8])

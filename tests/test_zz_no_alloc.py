@@ -44,6 +44,17 @@ def test_noalloc_matches_allocating_entry_point_twice():
     assert rel_l2(got_a2, want_a) <= TOL
 
 
+def test_noalloc_rows_without_a_radix_plan():
+    # 509 samples (prime): both entry points filter by circulant convolution with the
+    # inverse transform of the weights, kept in the static array after the weights
+    c = smooth_stack(2, 3, 509, seed=3)
+    want_c = T.apply_rweighting(c, 0.35, 0.05)
+    got_c = _noalloc(c, cutoff=0.35, falloff=0.05)
+    assert rel_l2(got_c, want_c) <= TOL
+    a = smooth_stack(5, 7, 512, seed=1)  # back to a radix plan: the convolution table is unused
+    assert rel_l2(_noalloc(a, cutoff=0.35, falloff=0.05), T.apply_rweighting(a, 0.35, 0.05)) <= TOL
+
+
 def test_noalloc_rejects_rows_beyond_the_static_limit():
     import torch
 
