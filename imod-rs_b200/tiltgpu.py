@@ -137,6 +137,7 @@ EXPORTS = {
     "tg_synth_projections": (C.c_int, [C.POINTER(PhantomSpec), _P, _P, _i32, _i32]),
     "tg_apply_rweighting_device_noalloc": (C.c_int, [_P, C.c_size_t, C.c_size_t, C.c_size_t, _f, _f,
                                                      _i32, _i32, _i32, _P]),
+    "tg_studio_reconstruct": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, _i32]),
     "tg_mrc_header_new": (C.c_int, [_i32, _i32, _i32, _i32, C.c_char_p, _P]),
     "tg_mrc_read": (C.c_int, [C.c_char_p, C.POINTER(MrcInfo), _i32, _i32, _P]),
     "tg_mrc_write_f32": (C.c_int, [C.c_char_p, _P, _P, _i32, _f, _f, _f]),
@@ -526,6 +527,12 @@ def apply_rweighting_device_noalloc(dev_ptr: int, nx, ny, nz, cutoff=0.35, fallo
     check(lib().tg_apply_rweighting_device_noalloc(_P(dev_ptr), nx, ny, nz, cutoff, falloff,
                                                    int(exact_filter_size or 0), int(use_hamming),
                                                    device, _P(stream or None)))
+
+
+def studio_reconstruct(ali_path, tlt_path, rec_path, device=0):
+    """imod-studio's reconstruction step (apps/imod-studio/src/main.rs:725-776) on the GPU."""
+    check(lib().tg_studio_reconstruct(str(ali_path).encode(), str(tlt_path).encode(), str(rec_path).encode(),
+                                      device))
 
 
 def synth_projections(angles, *, nx, ny, vol_nx=None, vol_nz, n_ell=300, rmin=3.0, rmax=40.0,

@@ -282,6 +282,17 @@ int tg_apply_rweighting_device_noalloc(float *dev_proj, size_t in_nx, size_t in_
                                        float cutoff, float falloff, int32_t exact_filter_size,
                                        int32_t use_hamming, int32_t device, void *cuda_stream);
 
+/* ---- imod-studio's reconstruction step ----
+ * Replaces step_reconstruction (apps/imod-studio/src/main.rs:725-776): reads the
+ * aligned stack (MRC) and tilt file, back-projects every row on the GPU without
+ * R-weighting or cosine stretch (zero fill, thickness = width, sum / sections;
+ * the tilt path with --no-weight --no-cosine-stretch --fill-mode zero -z nx)
+ * and writes the volume with MrcHeader::new(nx, nx, ny, Float), the label
+ * "imod-studio: reconstruction" and statistics (0, 0, 0), as the step does.
+ * TG_ERR_INVALID_ARG with "<path> not found" where the step returns that Err. */
+int tg_studio_reconstruct(const char *ali_path, const char *tlt_path, const char *rec_path,
+                          int32_t device);
+
 /* ---- Synthetic seeded inputs (no counterpart in the reference; the
  * workload generator for tests and benchmarks) ----
  * Projects a seeded random ellipsoid phantom (n_ell ellipsoids with semi-axes

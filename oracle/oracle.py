@@ -87,6 +87,7 @@ def lib():
             "or_output_stats32": (None, [P, i, i, i, f, f, f, P]),
             "or_wbp_rows32": (i, [P, P, P, i, i, i]),
             "or_wbp_rows64g": (i, [P, P, P, i, i, i]),
+            "or_studio_reconstruct32": (None, [P, i, i, i, P, i, P]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(_lib, name)
@@ -278,3 +279,14 @@ def wbp_rows(params: Params, proj: np.ndarray, y0: int, y1: int, nthreads=0, pre
     if rc != 0:
         raise RuntimeError(f"oracle wbp_rows failed with code {rc}")
     return vol
+
+
+def studio_reconstruct(proj: np.ndarray, angles) -> np.ndarray:
+    """imod-studio's reconstruction step (apps/imod-studio/src/main.rs:725-776):
+    returns [ny][nx][nx] float32."""
+    p = np.ascontiguousarray(proj, dtype=np.float32)
+    nz, ny, nx = p.shape
+    a = np.ascontiguousarray(angles, dtype=np.float32)
+    out = np.zeros((ny, nx, nx), np.float32)
+    lib().or_studio_reconstruct32(_ptr(p), nx, ny, nz, _ptr(a), len(a), _ptr(out))
+    return out

@@ -729,4 +729,38 @@ int or_wbp_rows64g(const or_params *p, const float *proj_in, double *vol_rows, i
   return wbp_rows<float, double>(p, proj_in, vol_rows, y0, y1, nt);
 }
 
+// The reconstruction step of imod-studio (apps/imod-studio/src/main.rs:725-776),
+// restated on its own: an unweighted back-projection with zero fill, thickness =
+// width, x = ((ox - cx) * cos + (oz - cz) * sin) + cx, the two-sample lerp only
+// when both samples are inside the row, and the sum scaled by 1/nz (f32, in the
+// reference's operation order).  out: [ny][nx (thickness)][nx].
+void or_studio_reconstruct32(const float *proj, int nx, int ny, int nz, const float *angles, int n_angles,
+                             float *out) {
+  const int out_nz = nx;
+  const float cx = (float)nx / 2.0f, cz = (float)out_nz / 2.0f;
+  const float pi = 3.14159265358979323846f;
+  for (int iy = 0; iy < ny; ++iy) {
+    float *sl = out + (size_t)iy * out_nz * nx;
+    for (size_t i = 0; i < (size_t)out_nz * nx; ++i) sl[i] = 0.0f;
+    for (int pi_ = 0; pi_ < n_angles && pi_ < nz; ++pi_) {
+      const float r = angles[pi_] * pi / 180.0f;
+      const float cos_t = cosf(r), sin_t = sinf(r);
+      const float *row = proj + ((size_t)pi_ * ny + iy) * nx;
+      for (int oz = 0; oz < out_nz; ++oz) {
+        const float bo = ((float)oz - cz) * sin_t;
+        for (int ox = 0; ox < nx; ++ox) {
+          const float px = ((float)ox - cx) * cos_t + bo + cx;
+          const long p0 = (long)floorf(px);
+          if (p0 >= 0 && p0 + 1 < nx) {
+            const float f = px - (float)p0;
+            sl[(size_t)oz * nx + ox] += row[p0] * (1.0f - f) + row[p0 + 1] * f;
+          }
+        }
+      }
+    }
+    const float inv = 1.0f / (float)nz;
+    for (size_t i = 0; i < (size_t)out_nz * nx; ++i) sl[i] *= inv;
+  }
+}
+
 }  // extern "C"

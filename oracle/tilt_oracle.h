@@ -114,6 +114,11 @@ int or_wbp_rows32(const or_params *p, const float *proj, float *vol_rows, int y0
 int or_wbp_rows64g(const or_params *p, const float *proj, double *vol_rows, int y0, int y1,
                    int nthreads);
 
+/* imod-studio's reconstruction step (apps/imod-studio/src/main.rs:725-776) restated
+ * directly: out[ny][nx][nx]. */
+void or_studio_reconstruct32(const float *proj, int nx, int ny, int nz, const float *angles,
+                             int n_angles, float *out);
+
 #ifdef __cplusplus
 }
 #endif

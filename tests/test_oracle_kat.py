@@ -208,3 +208,21 @@ def test_wbp_rows_equals_whole_run_slices(precision):
     whole, _ = O.run(p, proj, precision)
     rows = O.wbp_rows(p, proj, 3, 8, nthreads=4, precision=precision)
     np.testing.assert_array_equal(rows, whole[3:8])
+
+
+def test_studio_step_is_tilt_with_its_options():
+    # imod-studio's reconstruction step (apps/imod-studio/src/main.rs:725-776) is the
+    # tilt path with --no-weight --no-cosine-stretch --fill-mode zero and thickness = width:
+    # the same positions, lerp, skipped out-of-row samples (zero fill adds +0) and 1/nz
+    nz, ny, nx = 11, 5, 40
+    proj = random_stack(nz, ny, nx, seed=12, offset=-0.5)
+    ang = np.linspace(-55, 55, nz).astype(np.float32)
+    studio = O.studio_reconstruct(proj, ang)
+    p = O.Params(nx, ny, nz, ang, thickness=nx, no_weight=True, no_cosine_stretch=True, fill_mode="zero")
+    tilt, _ = O.run(p, proj, 32)
+    np.testing.assert_array_equal(studio, tilt)
+    # fewer angles than sections: the loop stops at the last angle, 1/nz still uses the sections
+    studio2 = O.studio_reconstruct(proj, ang[:7])
+    tilt2, _ = O.run(O.Params(nx, ny, nz, ang[:7], thickness=nx, no_weight=True, no_cosine_stretch=True,
+                              fill_mode="zero"), proj, 32)
+    np.testing.assert_array_equal(studio2, tilt2)
