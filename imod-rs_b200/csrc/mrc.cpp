@@ -150,6 +150,32 @@ static bool dims_reasonable(const Header &h) {
   return h.nx > 0 && h.ny > 0 && h.nz > 0 && h.nx < 100000 && h.ny < 100000 && h.nz < 1000000;
 }
 
+// IEEE 754 binary32 -> binary16, round to nearest, ties to even (the inverse of
+// f16_to_f32 below on every half value).  Mode-12 output: the reference reads
+// it (read.rs:468-499) but has no writer for it.
+uint16_t f32_to_f16(float f) {
+  uint32_t x;
+  memcpy(&x, &f, 4);
+  const uint32_t sign = (x >> 16) & 0x8000u, ax = x & 0x7fffffffu;
+  if (ax >= 0x7f800000u)  // infinity, or NaN (quiet, upper payload bits kept)
+    return (uint16_t)(sign | 0x7c00u | (ax > 0x7f800000u ? 0x200u | ((ax >> 13) & 0x3ffu) : 0u));
+  if (ax >= 0x477ff000u) return (uint16_t)(sign | 0x7c00u);  // >= 65520 rounds to infinity
+  if (ax < 0x38800000u) {  // below 2^-14: a subnormal half (or zero)
+    const int e = (int)(ax >> 23);
+    if (e < 102) return (uint16_t)sign;  // below 2^-25
+    const uint32_t m = (ax & 0x7fffffu) | 0x800000u;  // value = m * 2^(e-150), unit 2^-24
+    const int shift = 126 - e;                         // 14..24
+    uint32_t r = m >> shift;
+    const uint32_t rem = m & ((1u << shift) - 1u), half = 1u << (shift - 1);
+    if (rem > half || (rem == half && (r & 1u))) ++r;  // may carry into the smallest normal
+    return (uint16_t)(sign | r);
+  }
+  uint32_t r = ((((ax >> 23) - 127u + 15u) << 10) | ((ax & 0x7fffffu) >> 13));
+  const uint32_t rem = ax & 0x1fffu;
+  if (rem > 0x1000u || (rem == 0x1000u && (r & 1u))) ++r;  // a carry moves into the exponent
+  return (uint16_t)(sign | r);
+}
+
 float f16_to_f32(uint16_t bits) {  // crates/imod-mrc/src/read.rs:468-499
   uint32_t sign = (bits >> 15) & 1, exponent = (bits >> 10) & 0x1F, mant = bits & 0x3FF, out;
   if (exponent == 0) {
@@ -250,6 +276,17 @@ bool Reader::read_slice_f32(int z, std::vector<float> &out, std::string *err) {
   return true;
 }
 
+// write_slice_raw (write.rs:43-55): the bytes of one section in the file's mode
+bool Writer::write_slice_raw(const void *data, size_t bytes, std::string *err) {
+  if (bytes != h_.slice_bytes()) {
+    if (err) *err = "slice data size " + std::to_string(bytes) + " doesn't match expected " +
+                    std::to_string(h_.slice_bytes());
+    return false;
+  }
+  if (fwrite(data, 1, bytes, f_) != bytes) { if (err) *err = "write failed"; return false; }
+  return true;
+}
+
 bool Writer::create(const std::string &path, const Header &h, std::string *err) {
   f_ = fopen(path.c_str(), "wb");
   if (!f_) { if (err) *err = "cannot create " + path; return false; }
@@ -295,6 +332,13 @@ bool Writer::write_slice_f32(const float *data, size_t n, std::string *err) {
     case FLOAT:
       buf.resize(npix * 4);
       memcpy(buf.data(), data, npix * 4);  // little-endian host
+      break;
+    case HALF:  // addition: the reference reads mode 12 but does not write it
+      buf.resize(npix * 2);
+      for (size_t i = 0; i < npix; ++i) {
+        const uint16_t hb = f32_to_f16(data[i]);
+        memcpy(&buf[2 * i], &hb, 2);
+      }
       break;
     default:
       if (err) *err = "Unsupported MRC mode: " + std::to_string(h_.mode);

@@ -78,7 +78,9 @@ class Reader {
 class Writer {
  public:
   bool create(const std::string &path, const Header &h, std::string *err);
+  // write_slice_f32 (write.rs:58-104), plus mode 12 (IEEE half, round to nearest even)
   bool write_slice_f32(const float *data, size_t n, std::string *err);
+  bool write_slice_raw(const void *data, size_t bytes, std::string *err);
   bool finish(float amin, float amax, float amean, std::string *err);
   ~Writer();
 
@@ -88,6 +90,7 @@ class Writer {
 };
 
 float f16_to_f32(uint16_t bits);
+uint16_t f32_to_f16(float f);
 
 // read_tilt_file (crates/imod-transforms/src/tilt.rs:6-23)
 bool read_tilt_file(const std::string &path, std::vector<float> &angles, std::string *err);

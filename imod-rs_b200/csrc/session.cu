@@ -155,7 +155,7 @@ static void free_session(tg_session *s) {
   void *ptrs[] = {s->d_raw, s->d_logd, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_volh, s->d_maxbits, s->d_mpart, s->d_pairs,
                   s->d_part, s->d_slice_stats, s->d_stats3, s->d_vg, s->d_vg2, s->d_weights,
                   s->d_conv, s->d_stretch, s->d_tw, s->d_err, s->d_lvinfo, s->d_lgoff, s->d_lxs,
-                  s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab, s->d_xtb, s->d_lbnd};
+                  s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab, s->d_xtb, s->d_lbnd, s->d_half};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : s->ev)
@@ -169,7 +169,7 @@ void free_session_async(tg_session *s, cudaStream_t after) {
   void *ptrs[] = {s->d_raw, s->d_logd, s->d_means, s->d_vol, s->d_sino, s->d_tmp, s->d_volg, s->d_volh, s->d_maxbits, s->d_mpart, s->d_pairs,
                   s->d_part, s->d_slice_stats, s->d_stats3, s->d_vg, s->d_vg2, s->d_weights,
                   s->d_conv, s->d_stretch, s->d_tw, s->d_err, s->d_lvinfo, s->d_lgoff, s->d_lxs,
-                  s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab, s->d_xtb, s->d_lbnd};
+                  s->d_lys, s->d_lgdx, s->d_lgdy, s->d_ltab, s->d_xtb, s->d_lbnd, s->d_half};
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, after);
   for (auto &e : s->ev)
@@ -879,6 +879,50 @@ int tg_download_slices_async(tg_session *s, int32_t y0, int32_t y1, float *host_
   if (y1 > y0)
     TG_CUDA(cudaMemcpyAsync(host_out, s->d_vol + (size_t)y0 * sl, (size_t)(y1 - y0) * sl * 4,
                             cudaMemcpyDeviceToHost, s->st));
+  return TG_OK;
+}
+
+int tg_upload_sections(tg_session *s, int32_t z0, int32_t z1, const float *host) {
+  if (!s || z0 < 0 || z1 > s->nz || z0 > z1 || (!host && z1 > z0)) return TG_ERR_INVALID_ARG;
+  TG_CUDA(cudaSetDevice(s->dev));
+  const size_t sec = (size_t)s->nx * s->ny;
+  if (z1 > z0)
+    TG_CUDA(cudaMemcpyAsync(s->d_raw + (size_t)z0 * sec, host, (size_t)(z1 - z0) * sec * 4,
+                            cudaMemcpyHostToDevice, s->st));
+  s->uploaded = true;
+  return TG_OK;
+}
+
+int tg_download_slices_f16_async(tg_session *s, int32_t y0, int32_t y1, uint16_t *host_out) {
+  if (!s || y0 < 0 || y1 > s->ny || y0 > y1 || (!host_out && y1 > y0)) return TG_ERR_INVALID_ARG;
+  if (y1 == y0) return TG_OK;
+  TG_CUDA(cudaSetDevice(s->dev));
+  const size_t sl = (size_t)s->onx * s->onz, n = (size_t)(y1 - y0) * sl;
+  if (n * 2 > s->half_cap) {  // grows once for a caller's fixed chunk size
+    TG_CUDA(cudaStreamSynchronize(s->st));
+    if (s->d_half) cudaFree(s->d_half);
+    s->d_half = nullptr;
+    s->half_cap = 0;
+    cudaError_t e = cudaMalloc(&s->d_half, n * 2);
+    if (e != cudaSuccess) { s->d_half = nullptr; return cuda_fail(e, "cudaMalloc(half staging)"); }
+    s->half_cap = n * 2;
+  }
+  launch_to_half(s->d_vol + (size_t)y0 * sl, s->d_half, n, s->st);
+  TG_CUDA(cudaGetLastError());
+  TG_CUDA(cudaMemcpyAsync(host_out, s->d_half, n * 2, cudaMemcpyDeviceToHost, s->st));
+  return TG_OK;
+}
+
+int tg_host_alloc(size_t bytes, void **out) {
+  if (!out) return TG_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (bytes == 0) return TG_OK;
+  TG_CUDA(cudaHostAlloc(out, bytes, cudaHostAllocPortable));
+  return TG_OK;
+}
+
+int tg_host_free(void *p) {
+  if (p) TG_CUDA(cudaFreeHost(p));
   return TG_OK;
 }
 

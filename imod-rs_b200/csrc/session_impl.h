@@ -37,6 +37,8 @@ struct tg_session {  // one tilt series resident on a device
   double *d_mpart = nullptr;
   void *d_pairs = nullptr;
   size_t pairs_bytes = 0;
+  void *d_half = nullptr;   // mode-12 download staging (tg_download_slices_f16_async), grown on demand
+  size_t half_cap = 0;
   StatPartial *d_part = nullptr;
   float *d_slice_stats = nullptr, *d_stats3 = nullptr;
   float4 *d_vg = nullptr, *d_vg2 = nullptr;

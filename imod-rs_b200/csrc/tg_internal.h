@@ -175,6 +175,9 @@ void launch_transform_stats(float *vol, int onx, int onz, int ny, float dw, floa
 void launch_stats_reduce(const StatPartial *partial, int ny, int ntiles, int slice_count,
                          float *slice_stats, float *out3, cudaStream_t st);
 
+// f32 -> IEEE half (round to nearest even) of n values (mode-12 output)
+void launch_to_half(const float *in, void *out, size_t n, cudaStream_t st);
+
 // ---- synthetic data ----
 int synth_projections(const tg_phantom_spec *spec, const float *angles, float *d_out,
                       cudaStream_t st);

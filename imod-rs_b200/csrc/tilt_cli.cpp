@@ -13,6 +13,10 @@
 
 #include <algorithm>
 #include <cctype>
+#include <chrono>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
 #include <cerrno>
 #include <cstdio>
 #include <cstdlib>
@@ -48,6 +52,8 @@ struct Args {
   long fake_sirt = 0;
   std::string storage = "fp32";
   int device = 0;
+  int mode = 2;  // output MRC mode: 2 (float, the reference's) or 12 (half)
+  long io_chunk_kb = 128 * 1024;  // pinned staging chunk of the read and write pipelines
 };
 
 void usage(FILE *f) {
@@ -83,6 +89,9 @@ void usage(FILE *f) {
           "      --storage <fp32|fp16|bf16>   Staging precision of filtered projections (addition)\n"
           "      --device <N>                 CUDA device ordinal (addition)\n"
           "      --exact-xtilt                Per-view x-tilt row blend, bit-identical (addition)\n"
+          "      --mode <2|12>                Output MRC mode: 2 float, 12 half (addition) [default: 2]\n"
+          "      --io-chunk-kb <N>            Staging chunk of the overlapped read/write (addition)\n"
+          "                                   [default: 131072]\n"
           "  -h, --help                       Print help\n\n"
           "PIP-style aliases (additions): -InputProjections -OutputFile -TILTFILE -THICKNESS\n"
           "  -WIDTH -RADIAL -SIRTIterations -LOG -SCALE <add,mult> -FakeSIRTiterations\n"
@@ -193,6 +202,11 @@ Args parse(int argc, char **argv) {
     else if (name == "fake-sirt") a.fake_sirt = parse_int(val, "--fake-sirt", false);
     else if (name == "storage") a.storage = lower(val);
     else if (name == "device") a.device = (int)parse_int(val, "--device", false);
+    else if (name == "io-chunk-kb") a.io_chunk_kb = std::max(1L, parse_int(val, "--io-chunk-kb", false));
+    else if (name == "mode") {
+      a.mode = (int)parse_int(val, "--mode", false);
+      if (a.mode != 2 && a.mode != 12) clap_error("invalid value '" + val + "' for '--mode': 2 or 12");
+    }
     else if (name == "SCALE") {  // IMOD: (v + add) * mult == (v * mult) + add*mult
       size_t c = val.find(',');
       float add = parse_float(val.substr(0, c), "-SCALE");
@@ -251,14 +265,6 @@ int main(int argc, char **argv) {
     float v;
     if (parts.size() > 0 && mrc::parse_f32(tr(parts[0]), v)) cutoff = v;
     if (parts.size() > 1 && mrc::parse_f32(tr(parts[1]), v)) falloff = v;
-  }
-  std::vector<float> proj((size_t)in_nx * in_ny * nz), sl;
-  for (int z = 0; z < nz; ++z) {
-    if (!reader.read_slice_f32(z, sl, &err) || sl.size() != (size_t)in_nx * in_ny) {
-      fprintf(stderr, "Error: %s\n", err.empty() ? "unsupported slice layout" : err.c_str());
-      return 1;
-    }
-    std::copy(sl.begin(), sl.end(), proj.begin() + (size_t)z * in_nx * in_ny);
   }
   std::vector<float> local_rows, xtilt, zfac;
   if (!args.local_file.empty() && !mrc::load_local_rows(args.local_file, local_rows, &err)) {
@@ -321,41 +327,146 @@ int main(int argc, char **argv) {
     fprintf(stderr, "Error: %s (%s)\n", tg_status_string(rc), tg_last_error());
     return 1;
   }
-  if ((rc = tg_upload_projections(s, proj.data(), proj.size())) != TG_OK || (rc = tg_reconstruct(s)) != TG_OK ||
-      (rc = tg_synchronize(s)) != TG_OK) {
-    fprintf(stderr, "Error: %s (%s)\n", tg_status_string(rc), tg_last_error());
+  auto fail = [&](int r) {
+    fprintf(stderr, "Error: %s (%s)\n", tg_status_string(r), tg_last_error());
     tg_session_destroy(s);
     return 1;
+  };
+  using clk = std::chrono::steady_clock;
+  auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
+  const auto t_read0 = clk::now();
+  // ---- input: a reader thread fills two pinned chunks of sections (read_slice_f32,
+  // read.rs:127-231) while the previous chunk is copied to the device
+  const size_t sec = (size_t)in_nx * in_ny;
+  const size_t chunk_bytes = (size_t)args.io_chunk_kb << 10;
+  const int zc = std::max(1, (int)std::min<size_t>((size_t)nz, chunk_bytes / (sec * 4)));
+  void *pin_in[2] = {nullptr, nullptr};
+  for (auto &p : pin_in)
+    if ((rc = tg_host_alloc((size_t)zc * sec * 4, &p)) != TG_OK) return fail(rc);
+  {
+    std::mutex mu;
+    std::condition_variable cv;
+    int filled[2] = {-1, -1};  // chunk index held by each slot, -1: free
+    bool read_failed = false, stop = false;  // stop: the uploader gave up, the reader quits
+    std::string read_err;
+    const int nchunks = (nz + zc - 1) / zc;
+    std::thread rd([&] {
+      std::vector<float> sl;
+      std::string e;
+      for (int k = 0; k < nchunks; ++k) {
+        {
+          std::unique_lock<std::mutex> lk(mu);
+          cv.wait(lk, [&] { return filled[k % 2] < 0 || stop; });
+          if (stop) return;
+        }
+        float *dst = static_cast<float *>(pin_in[k % 2]);
+        const int z0 = k * zc, z1 = std::min(nz, z0 + zc);
+        for (int z = z0; z < z1; ++z) {
+          if (!reader.read_slice_f32(z, sl, &e) || sl.size() != sec) {
+            std::lock_guard<std::mutex> lk(mu);
+            read_failed = true;
+            read_err = e.empty() ? "unsupported slice layout" : e;
+            filled[k % 2] = k;
+            cv.notify_all();
+            return;
+          }
+          std::copy(sl.begin(), sl.end(), dst + (size_t)(z - z0) * sec);
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        filled[k % 2] = k;
+        cv.notify_all();
+      }
+    });
+    int up_rc = TG_OK;
+    for (int k = 0; k < nchunks; ++k) {
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return filled[k % 2] == k; });
+        if (read_failed) break;
+      }
+      const int z0 = k * zc, z1 = std::min(nz, z0 + zc);
+      if ((up_rc = tg_upload_sections(s, z0, z1, static_cast<float *>(pin_in[k % 2]))) == TG_OK)
+        up_rc = tg_synchronize(s);  // the slot may be refilled once its copy is done
+      std::lock_guard<std::mutex> lk(mu);
+      filled[k % 2] = -1;
+      if (up_rc != TG_OK) stop = true;
+      cv.notify_all();
+      if (up_rc != TG_OK) break;
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (read_failed) stop = true;
+      cv.notify_all();
+    }
+    rd.join();
+    for (auto &p : pin_in) tg_host_free(p);
+    if (up_rc != TG_OK) return fail(up_rc);
+    if (read_failed) {
+      fprintf(stderr, "Error: %s\n", read_err.c_str());
+      tg_session_destroy(s);
+      return 1;
+    }
   }
+  const auto t_rec0 = clk::now();
+  if ((rc = tg_reconstruct(s)) != TG_OK || (rc = tg_synchronize(s)) != TG_OK) return fail(rc);
+  const auto t_rec1 = clk::now();
   uint8_t hin[1024], hout[1024];  // main.rs:710-717
   h.to_bytes(hin, false);
   tg_tilt_output_header(hin, out_nx, out_nz, hout);
   mrc::Header oh = mrc::Header::from_bytes(hout, false);
+  if (args.mode == 12) oh.mode = mrc::HALF;
   mrc::Writer w;
   if (!w.create(args.output, oh, &err)) {
     fprintf(stderr, "Error: %s\n", err.c_str());
     tg_session_destroy(s);
     return 1;
   }
+  // ---- output: chunk k+1 is copied off the device into one pinned buffer while
+  // chunk k is written from the other (the reference writes each slice as it is
+  // made, main.rs:1077-1085)
   const size_t slice = (size_t)out_nx * out_nz;
-  const int chunk = std::max(1, (int)std::min<size_t>(64, (256u << 20) / (slice * 4)));
-  std::vector<float> buf((size_t)chunk * slice);
+  const size_t eb = args.mode == 12 ? 2 : 4;
+  const int chunk = std::max(1, (int)std::min<size_t>((size_t)out_ny, chunk_bytes / (slice * eb)));
+  void *pin_out[2] = {nullptr, nullptr};
+  for (auto &p : pin_out)
+    if ((rc = tg_host_alloc((size_t)chunk * slice * eb, &p)) != TG_OK) return fail(rc);
+  auto queue = [&](int y0, void *dst) {
+    const int y1 = std::min(out_ny, y0 + chunk);
+    return args.mode == 12 ? tg_download_slices_f16_async(s, y0, y1, static_cast<uint16_t *>(dst))
+                           : tg_download_slices_async(s, y0, y1, static_cast<float *>(dst));
+  };
   tg_stats st{};
-  for (int y0 = 0; y0 < out_ny; y0 += chunk) {
-    int y1 = std::min(out_ny, y0 + chunk);
-    if ((rc = tg_download_slices(s, y0, y1, buf.data(), &st)) != TG_OK) {
-      fprintf(stderr, "Error: %s (%s)\n", tg_status_string(rc), tg_last_error());
-      tg_session_destroy(s);
-      return 1;
-    }
-    for (int y = y0; y < y1; ++y)
-      if (!w.write_slice_f32(buf.data() + (size_t)(y - y0) * slice, slice, &err)) {
+  rc = tg_get_stats(s, &st);
+  int k = 0;
+  if (rc == TG_OK) rc = queue(0, pin_out[0]);
+  for (int y0 = 0; rc == TG_OK && y0 < out_ny; y0 += chunk, ++k) {
+    if ((rc = tg_synchronize(s)) != TG_OK) break;  // chunk k is in pin_out[k % 2]
+    if (y0 + chunk < out_ny && (rc = queue(y0 + chunk, pin_out[(k + 1) % 2])) != TG_OK) break;
+    const int y1 = std::min(out_ny, y0 + chunk);
+    const uint8_t *src = static_cast<const uint8_t *>(pin_out[k % 2]);
+    for (int y = y0; y < y1; ++y) {
+      const bool ok = args.mode == 12 ? w.write_slice_raw(src + (size_t)(y - y0) * slice * 2, slice * 2, &err)
+                                      : w.write_slice_f32(reinterpret_cast<const float *>(src) + (size_t)(y - y0) * slice,
+                                                          slice, &err);
+      if (!ok) {
         fprintf(stderr, "Error: %s\n", err.c_str());
+        tg_synchronize(s);
+        for (auto &p : pin_out) tg_host_free(p);
         tg_session_destroy(s);
         return 1;
       }
+    }
     fprintf(stderr, "  %d/%d rows\n", y1, out_ny);
   }
+  if (rc != TG_OK) {
+    tg_synchronize(s);
+    for (auto &p : pin_out) tg_host_free(p);
+    return fail(rc);
+  }
+  for (auto &p : pin_out) tg_host_free(p);
+  const auto t_wr1 = clk::now();
+  fprintf(stderr, "tilt: read+upload %.3f s, reconstruct %.3f s, download+write %.3f s\n", secs(t_read0, t_rec0),
+          secs(t_rec0, t_rec1), secs(t_rec1, t_wr1));
   tg_run_info info{};
   tg_session_last_run(s, &info);
   tg_session_destroy(s);

@@ -7,6 +7,10 @@
 //     and an f64 sum; the header mean is sum_slices(f32 slice mean as f64 *
 //     slice size) / total.  Partial sums are per (slice, tile) and reduced in a
 //     fixed order, so the statistics are deterministic.
+#include <cuda_fp16.h>
+
+#include <algorithm>
+
 #include "tg_internal.h"
 
 namespace tg {
@@ -150,6 +154,41 @@ void launch_stats_reduce(const StatPartial *partial, int ny, int ntiles, int cou
                          float *slice_stats, float *out3, cudaStream_t st) {
   slice_stats_kernel<<<ny, 256, 0, st>>>(partial, ntiles, count, slice_stats);
   fold_slices_kernel<<<1, 1, 0, st>>>(slice_stats, ny, count, out3);
+}
+
+// f32 -> IEEE half, round to nearest even, for mode-12 output (n values).  With
+// both pointers 16-byte aligned each thread converts 8 values per step; otherwise
+// (a slice range whose start is not a multiple of 4 values) one per step.
+template <bool VEC>
+__global__ void __launch_bounds__(256) to_half_kernel(const float *__restrict__ in, __half *__restrict__ out,
+                                                      size_t n) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x, t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!VEC) {
+    for (size_t i = t0; i < n; i += stride) out[i] = __float2half_rn(__ldcs(in + i));
+    return;
+  }
+  const size_t n8 = n / 8;
+  for (size_t i = t0; i < n8; i += stride) {
+    const float4 a = __ldcs(reinterpret_cast<const float4 *>(in) + 2 * i);
+    const float4 b = __ldcs(reinterpret_cast<const float4 *>(in) + 2 * i + 1);
+    const __half2 h0 = __floats2half2_rn(a.x, a.y), h1 = __floats2half2_rn(a.z, a.w);
+    const __half2 h2 = __floats2half2_rn(b.x, b.y), h3 = __floats2half2_rn(b.z, b.w);
+    uint4 w;
+    w.x = *reinterpret_cast<const uint32_t *>(&h0);
+    w.y = *reinterpret_cast<const uint32_t *>(&h1);
+    w.z = *reinterpret_cast<const uint32_t *>(&h2);
+    w.w = *reinterpret_cast<const uint32_t *>(&h3);
+    reinterpret_cast<uint4 *>(out)[i] = w;
+  }
+  if (t0 < n - 8 * n8) out[8 * n8 + t0] = __float2half_rn(in[8 * n8 + t0]);
+}
+
+void launch_to_half(const float *in, void *out, size_t n, cudaStream_t st) {
+  if (n == 0) return;
+  const bool vec = ((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0);
+  const size_t blocks = std::min<size_t>((n / (vec ? 8 : 1) + 255) / 256 + 1, 148 * 8);
+  if (vec) to_half_kernel<true><<<(unsigned)blocks, 256, 0, st>>>(in, static_cast<__half *>(out), n);
+  else to_half_kernel<false><<<(unsigned)blocks, 256, 0, st>>>(in, static_cast<__half *>(out), n);
 }
 
 }  // namespace tg

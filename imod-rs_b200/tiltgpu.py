@@ -138,6 +138,10 @@ EXPORTS = {
     "tg_apply_rweighting_device_noalloc": (C.c_int, [_P, C.c_size_t, C.c_size_t, C.c_size_t, _f, _f,
                                                      _i32, _i32, _i32, _P]),
     "tg_studio_reconstruct": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, _i32]),
+    "tg_upload_sections": (C.c_int, [_P, _i32, _i32, _P]),
+    "tg_download_slices_f16_async": (C.c_int, [_P, _i32, _i32, _P]),
+    "tg_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_P)]),
+    "tg_host_free": (C.c_int, [_P]),
     "tg_mrc_header_new": (C.c_int, [_i32, _i32, _i32, _i32, C.c_char_p, _P]),
     "tg_mrc_read": (C.c_int, [C.c_char_p, C.POINTER(MrcInfo), _i32, _i32, _P]),
     "tg_mrc_write_f32": (C.c_int, [C.c_char_p, _P, _P, _i32, _f, _f, _f]),

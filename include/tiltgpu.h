@@ -138,6 +138,24 @@ int tg_download_slices(tg_session *s, int32_t y0, int32_t y1, float *host_out, t
  * caller keeps host_out alive and calls tg_synchronize before reading it.
  * Lets one series' download overlap the next series' upload and compute. */
 int tg_download_slices_async(tg_session *s, int32_t y0, int32_t y1, float *host_out);
+/* Queues the copy of sections (views) [z0, z1) ([view][row][x] floats) from host
+ * memory into the session on its stream and returns at once: the caller keeps
+ * `host` unchanged until tg_synchronize, then may reuse it.  Lets a reader
+ * stream a stack in as MrcReader::read_slice_f32 produces it
+ * (crates/imod-mrc/src/read.rs:127-231, apps/tilt/src/main.rs:602-605); every
+ * section must be uploaded before tg_reconstruct. */
+int tg_upload_sections(tg_session *s, int32_t z0, int32_t z1, const float *host);
+/* Queues output slices [y0, y1) converted on the device to IEEE half (round to
+ * nearest even) into host_out (2 bytes per voxel, little-endian), for MRC mode
+ * 12 output at half the bytes.  The reference reads mode 12
+ * (crates/imod-mrc/src/read.rs:468-499) but its write_slice_f32
+ * (write.rs:58-104) has no half case; this is an addition.  Values beyond the
+ * half range become infinities.  Synchronise before reading host_out. */
+int tg_download_slices_f16_async(tg_session *s, int32_t y0, int32_t y1, uint16_t *host_out);
+/* Page-locked host memory (cudaHostAlloc), for copies that overlap with other
+ * work; free with tg_host_free.  No counterpart in the reference. */
+int tg_host_alloc(size_t bytes, void **out);
+int tg_host_free(void *p);
 int tg_get_stats(tg_session *s, tg_stats *stats);
 /* Device pointer of the resident volume [ny][out_nz][out_nx]. */
 const float *tg_volume_device(tg_session *s);

@@ -83,3 +83,9 @@ def test_no_gpu_is_an_error_not_a_fallback(tmp_path):
     r = run("-i", m, "-o", tmp_path / "o.mrc", "-t", t)
     assert r.returncode == 1 and "no sm_100 CUDA device" in r.stderr
     assert not os.path.exists(tmp_path / "o.mrc")
+
+
+def test_mode_flag_accepts_2_and_12_only():
+    r = run("-i", "a", "-o", "b", "-t", "c", "--mode", "4")
+    assert r.returncode == 2 and "--mode" in r.stderr
+    assert "--mode" in run("--help").stdout and "--io-chunk-kb" in run("--help").stdout

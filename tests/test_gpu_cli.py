@@ -48,3 +48,29 @@ def test_tilt_cli_matches_oracle(tmp_path, extra, okw):
     tol = 2e-3 if "fp16" in extra else 1e-5
     assert rel_l2(vol.reshape(ref.shape), ref) <= tol
     assert abs(info.amean - rst["amean"]) <= 10 * tol * max(1.0, abs(rst["amean"]))
+
+
+@pytest.mark.parametrize("chunk_kb", [131072, 4])
+def test_tilt_cli_mode_12_and_chunked_io(tmp_path, chunk_kb):
+    # --mode 12 (an addition: half output at half the bytes, readable by the reference's
+    # read_slice_f32) must equal the float output rounded to nearest even; a 4 KB staging
+    # chunk makes both the read and the write pipelines take many chunks
+    nz, ny, nx, thick = 17, 9, 64, 30
+    proj = (smooth_stack(nz, ny, nx, seed=62) * 100.0).astype(np.float32)
+    ang = np.linspace(-54, 54, nz).astype(np.float32)
+    src, tlt = tmp_path / "in.mrc", tmp_path / "in.tlt"
+    T.mrc_write_f32(src, T.mrc_header_new(nx, ny, nz, "Float"), proj)
+    T.write_tilt_file(tlt, ang)
+    outs = {}
+    for mode in (2, 12):
+        out = tmp_path / f"out{mode}.rec"
+        r = run("-i", src, "-o", out, "-t", tlt, "-z", thick, "--mode", mode, "--io-chunk-kb", chunk_kb)
+        assert r.returncode == 0, r.stderr
+        outs[mode] = T.mrc_read(out)
+    i2, v2 = outs[2]
+    i12, v12 = outs[12]
+    assert i12.mode == 12 and (i12.nx, i12.ny, i12.nz) == (i2.nx, i2.ny, i2.nz)
+    assert (i12.amin, i12.amax, i12.amean) == (i2.amin, i2.amax, i2.amean)
+    np.testing.assert_array_equal(v12, v2.astype(np.float16).astype(np.float32))
+    ref, _ = O.run(O.Params(nx, ny, nz, ang, thickness=thick), proj, 32)
+    assert rel_l2(v2.reshape(ref.shape), ref) <= 1e-5

@@ -222,3 +222,24 @@ def test_tilt_output_header():
     assert out["ylen"] == np.float32(np.float32(250.0) * np.float32(30) / np.float32(100))
     assert out["zlen"] == 200.0 and out["nlabl"] == 1
     assert out["labels"][:80].decode() == "tilt: 41 projections, thickness 30".ljust(80)
+
+
+def test_write_mode_12_rounds_to_nearest_even(tmp_path):
+    # the writer's f32 -> half conversion (an addition: the reference reads mode 12,
+    # crates/imod-mrc/src/read.rs:468-499, but does not write it) against numpy's IEEE
+    # round-to-nearest-even: normals, ties, subnormals, the largest half, overflow
+    rng = np.random.default_rng(12)
+    specials = np.array([0.0, -0.0, 1.0, -2.5, 65504.0, 65519.99, 65520.0, -7e4, 1e-8, 2.9802322e-08,
+                         5.9604645e-08, 8.940697e-08, 6.1035156e-05, 6.097e-05, 1.0009766, 1.00146484,
+                         np.inf, -np.inf, 3.0e-6], np.float32)
+    vals = np.concatenate([specials, rng.standard_normal(4000).astype(np.float32) * 10.0 ** rng.integers(-9, 6, 4000)])
+    vals = vals.astype(np.float32)
+    n = len(vals)
+    p = tmp_path / "w12.mrc"
+    T.mrc_write_f32(p, T.mrc_header_new(n, 1, 1, "HalfFloat"), vals)
+    info, back = T.mrc_read(p)
+    assert info.mode == 12 and os.path.getsize(p) == 1024 + 2 * n
+    with np.errstate(over="ignore"):
+        want = vals.astype(np.float16)
+    np.testing.assert_array_equal(np.fromfile(p, "<u2", offset=1024), want.view("<u2"))
+    np.testing.assert_array_equal(back, want.astype(np.float32))
