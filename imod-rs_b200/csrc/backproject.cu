@@ -178,15 +178,16 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;  // 2 s: a stage never legitimately takes this long
-// Bounded wait on an mbarrier phase: sleeps in try_wait, gives up after
-// WAIT_LIMIT_NS of wall time or when another warp of the CTA has given up.
-__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t parity, volatile int *abort) {
+// Bounded wait on an mbarrier phase: sleeps in try_wait, gives up after limit_ns
+// of wall time (BpArgs::wait_limit_ns, 2 s by default: a stage never
+// legitimately takes that long) or, when abort is given, as soon as another warp
+// of the CTA has given up.
+__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t parity, volatile int *abort, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   for (;;) {
     if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
-    if (*abort || globaltimer_ns() - t0 > WAIT_LIMIT_NS) return false;
+    if ((abort && *abort) || globaltimer_ns() - t0 > limit_ns) return false;
   }
 }
 
@@ -214,10 +215,14 @@ template <class C> struct SmemLayout {
 // One output tile (S slices x TX columns x TZ depths) of one series.  gst is the
 // CTA's running stage count: ring slots and mbarrier phases continue across the
 // tiles a persistent CTA processes.  Returns false on abort.
+// Producer state that outlives a tile: issued = 1 + the global index of the last
+// stage whose copies were issued; skipped = a stage left out by the test hook (-1).
+struct ProducerState { int issued = 0, skipped = -1; };
+
 template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
 __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz, unsigned char *sm,
                                         const SmemLayout<FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>> &L,
-                                        int &gst, volatile int *s_abort_p) {
+                                        int &gst, volatile int *s_abort_p, ProducerState &ps) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   constexpr int SP = C::SP, OZG = C::OZG, TZ = C::TZ, EB = C::EB, WMAX = C::WMAX, SLOT = C::SLOT;
   unsigned char *bufs = L.bufs;
@@ -274,11 +279,18 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
     const int jp0 = iy0 / 2;
     for (int st = 0; st < nst; ++st) {
       const int g = g0 + st, b = g % NSTAGE;
-      if (g >= NSTAGE && !wait_phase(smem_u32(&empty[b]), ((g / NSTAGE) - 1) & 1, &s_abort)) {
-        s_abort = 1;
+      bool go = g < NSTAGE || wait_phase(smem_u32(&empty[b]), ((g / NSTAGE) - 1) & 1, &s_abort, a.wait_limit_ns);
+      // one decision for the whole warp: no lane may leave while others reach the
+      // warp-wide reduction below
+      go = __all_sync(0xffffffffu, go && !s_abort);
+      if (!go) {
+        if (lane == 0) s_abort = 1;
         return false;
       }
-      if (s_abort) return false;
+      if (st == a.fault_skip_stage) {  // test hook: no expect_tx, no copy -> full[b] never completes
+        ps.skipped = g;
+        continue;
+      }
       const int v0 = st * VPS, nv = min(VPS, a.nviews - v0);
       const bool mine = lane < nv * SP;
       const int vi = lane / SP, sp = lane % SP, v = v0 + vi;
@@ -295,6 +307,7 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
         const uint32_t dst = smem_u32(bufs) + (b * VPS + vi) * SLOT + sp * WMAX * EB;
         bulk_g2s(dst, src, bytes, smem_u32(&full[b]));
       }
+      ps.issued = g + 1;
     }
     return true;
   }
@@ -323,7 +336,7 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
   bool ok = true;
   for (int st = 0; st < nst && ok; ++st) {
     const int g = g0 + st, b = g % NSTAGE;
-    if (!wait_phase(smem_u32(&full[b]), (g / NSTAGE) & 1, &s_abort)) {
+    if (!wait_phase(smem_u32(&full[b]), (g / NSTAGE) & 1, &s_abort, a.wait_limit_ns)) {
       s_abort = 1;
       ok = false;
       break;
@@ -392,6 +405,7 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
     __syncwarp();
     if ((tid & 31) == 0) mbar_arrive(smem_u32(&empty[b]));  // this warp is done with buffer b
   }
+  __syncwarp();       // lanes that left the loop at different stages reconverge
   consumer_sync(NT);  // all consumers past the loop (buffers free, abort flag settled)
   if (s_abort) {
     if (tid == 0) atomicOr(a.err, 1);
@@ -481,12 +495,15 @@ template <class C> __device__ __forceinline__ void init_ring(const SmemLayout<C>
 }
 
 // The producer leaves no copy landing in shared memory after the CTA exits
-// (only possible after an abort): bounded wait on the last NSTAGE stages.
-template <class C> __device__ __forceinline__ void drain_ring(const SmemLayout<C> &L, int gst,
-                                                              volatile int *s_abort) {
+// (only possible after an abort): a bounded wait, which an abort does not cut
+// short, on each of the last NSTAGE stages it issued (a stage it left out by the
+// test hook has no copy in flight).  Within the last NSTAGE issued stages every
+// barrier serves one stage, so its parity identifies that stage's phase.
+template <class C> __device__ __forceinline__ void drain_ring(const SmemLayout<C> &L, const ProducerState &ps,
+                                                              volatile int *s_abort, uint64_t limit_ns) {
   if (threadIdx.x == C::NT_ && *s_abort)
-    for (int g = max(0, gst - C::NSTAGE_); g < gst; ++g)
-      wait_phase(smem_u32(&L.full[g % C::NSTAGE_]), (g / C::NSTAGE_) & 1, s_abort);
+    for (int g = max(0, ps.issued - C::NSTAGE_); g < ps.issued; ++g)
+      if (g != ps.skipped) wait_phase(smem_u32(&L.full[g % C::NSTAGE_]), (g / C::NSTAGE_) & 1, nullptr, limit_ns);
 }
 
 // One launch per series: grid = tiles of that series.
@@ -498,8 +515,9 @@ __global__ void __launch_bounds__(NT + 32) bp_fast_kernel(const __grid_constant_
   const SmemLayout<C> L(sm, a.nviews);
   init_ring(L, &s_abort);
   int gst = 0;
-  bp_tile<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>(a, blockIdx.x, blockIdx.y, blockIdx.z, sm, L, gst, &s_abort);
-  drain_ring(L, gst, &s_abort);
+  ProducerState ps;
+  bp_tile<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>(a, blockIdx.x, blockIdx.y, blockIdx.z, sm, L, gst, &s_abort, ps);
+  drain_ring(L, ps, &s_abort, a.wait_limit_ns);
 }
 
 // Persistent launch over the tiles of many series: each CTA takes the next
@@ -517,6 +535,8 @@ __global__ void __launch_bounds__(NT + 32) bp_batch_kernel(const BpArgs *__restr
   const SmemLayout<C> L(sm, max_views);
   init_ring(L, &s_abort);
   int gst = 0;
+  ProducerState ps;
+  uint64_t limit_ns = 2000000000ull;
   for (;;) {
     if (threadIdx.x == 0) {
       const int t = atomicAdd(counter, 1);
@@ -539,11 +559,12 @@ __global__ void __launch_bounds__(NT + 32) bp_batch_kernel(const BpArgs *__restr
     __syncthreads();
     const int nbx = s_args.nbx, nxz = s_args.ntiles_xz;
     const int bx = T.z % nbx, by = (T.z % nxz) / nbx, bz = T.z / nxz;
-    if (!bp_tile<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>(s_args, bx, by, bz, sm, L, gst, &s_abort)) {
+    limit_ns = s_args.wait_limit_ns;
+    if (!bp_tile<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>(s_args, bx, by, bz, sm, L, gst, &s_abort, ps)) {
       s_abort = 1;
     }
   }
-  drain_ring(L, gst, &s_abort);
+  drain_ring(L, ps, &s_abort, limit_ns);
 }
 
 

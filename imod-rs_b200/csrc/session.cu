@@ -283,6 +283,8 @@ BpArgs bp_args(tg_session *s, int mode) {
   a.mode = mode;
   a.has_local = s->has_local ? 1 : 0;
   a.loc = local_dev(s);
+  a.wait_limit_ns = s->wait_limit_ns;
+  a.fault_skip_stage = s->fault_skip_stage;
   return a;
 }
 
@@ -347,6 +349,8 @@ int autotune(tg_session *s) {
   TG_CUDA(cudaEventCreate(&e1));
   for (int v = 0; v < bp_fast_variants(); ++v) {
     BpArgs a = bp_args(s, 1);
+    a.wait_limit_ns = 2000000000ull;  // tuning never runs the test hook
+    a.fault_skip_stage = -1;
     if (s->xt_split) a.vol = s->xtb;
     int nt = 0;
     // warm + timed launch (mode 1 writes the volume, which is rewritten afterwards)
@@ -982,6 +986,23 @@ int tg_session_kernel_info(tg_session *s, int32_t *fast, int32_t *variant, int32
   if (fmt) *fmt = s->fmt;
   if (padL) *padL = s->padL;
   if (PW) *PW = s->PW;
+  return TG_OK;
+}
+
+int tg_session_inject_wait_fault(tg_session *s, int32_t skip_stage, uint32_t wait_limit_us) {
+  if (!s) return TG_ERR_INVALID_ARG;
+  if (!s->fast && !s->xt_split) {
+    set_error("the session does not use the pipelined back-projector");
+    return TG_ERR_UNSUPPORTED;
+  }
+  TG_CUDA(cudaSetDevice(s->dev));
+  TG_CUDA(cudaStreamSynchronize(s->st));
+  s->fault_skip_stage = skip_stage < 0 ? -1 : skip_stage;
+  s->wait_limit_ns = wait_limit_us ? (unsigned long long)wait_limit_us * 1000ull : 2000000000ull;
+  if (s->sirt_exec) {  // captured iterations hold the old arguments: capture again
+    cudaGraphExecDestroy(s->sirt_exec);
+    s->sirt_exec = nullptr;
+  }
   return TG_OK;
 }
 

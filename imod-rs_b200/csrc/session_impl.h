@@ -58,6 +58,9 @@ struct tg_session {  // one tilt series resident on a device
   tg_run_info info{};
   cudaEvent_t ev[6] = {};
   cudaGraphExec_t sirt_exec = nullptr;
+  // bounded-wait settings of the fast back-projector (tg_session_inject_wait_fault)
+  unsigned long long wait_limit_ns = 2000000000ull;
+  int fault_skip_stage = -1;
   int iter_launches = 0;  // kernels of one SIRT iteration
   float cx = 0, cz = 0, ocx = 0, inv_n = 0;
   cudaMemPool_t pool = nullptr;  // stream-ordered allocations (server sessions)

@@ -95,6 +95,12 @@ struct BpArgs {
   LocalDev loc;
   int nbx, ntiles_xz;       // tile grid of the fast kernel (set by its launcher)
   int tile0;                // batched launch: index of this series' first tile
+  // bounded pipeline waits of the fast kernel: give up after wait_limit_ns (error bit 0)
+  unsigned long long wait_limit_ns;
+  // test hook (tg_session_inject_wait_fault): the producer issues no copy for this
+  // stage of each tile, so the consumers' wait on it runs out; -1: none
+  int fault_skip_stage;
+  int pad_;
 };
 // A persistent back-projection launch over the tiles of several series.  Tile t
 // belongs to the series j with jobs[j].tile0 <= t < jobs[j+1].tile0 (series in

@@ -139,6 +139,7 @@ EXPORTS = {
                                                      _i32, _i32, _i32, _P]),
     "tg_studio_reconstruct": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, _i32]),
     "tg_upload_sections": (C.c_int, [_P, _i32, _i32, _P]),
+    "tg_session_inject_wait_fault": (C.c_int, [_P, _i32, C.c_uint32]),
     "tg_download_slices_f16_async": (C.c_int, [_P, _i32, _i32, _P]),
     "tg_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_P)]),
     "tg_host_free": (C.c_int, [_P]),
@@ -305,6 +306,11 @@ class Session:
             name = lib().tg_variant_name(variant).decode() + ("+xtilt-blend" if fast == 3 else "")
         return {"fast": fast == 1, "xtilt_split": fast == 3, "variant": variant,
                 "variant_name": name, "fmt": fmt, "padL": padl, "PW": pw}
+
+    def inject_wait_fault(self, skip_stage=-1, wait_limit_us=0):
+        """Test hook: the back-projector's producer leaves out one pipeline stage and
+        its bounded waits give up after wait_limit_us (see tiltgpu.h)."""
+        check(lib().tg_session_inject_wait_fault(self.h, int(skip_stage), int(wait_limit_us)))
 
     def set_variant(self, v: int):
         check(lib().tg_session_set_variant(self.h, v))

@@ -169,6 +169,15 @@ size_t tg_session_device_bytes(tg_session *s);
  * reference (its wgpu queue is private); lets a host runtime order the work
  * with its own copies and timers. */
 int tg_session_set_stream(tg_session *s, void *cuda_stream);
+/* Test hook of the bounded device waits (no counterpart in the reference).  The
+ * pipelined back-projector's waits give up after wait_limit_us (0: the default
+ * 2 s) and report TG_ERR_TIMEOUT through tg_synchronize.  skip_stage >= 0 makes
+ * its producer issue no copy for that pipeline stage of every tile, so the
+ * consumers' bounded wait on it runs out: the timeout path runs without any
+ * device fault, and the session stays usable (skip_stage -1 and wait_limit_us 0
+ * restore normal operation).  TG_ERR_UNSUPPORTED for sessions that do not use
+ * that back-projector (local alignment, per-view x-tilts). */
+int tg_session_inject_wait_fault(tg_session *s, int32_t skip_stage, uint32_t wait_limit_us);
 int tg_session_destroy(tg_session *s);
 
 /* ---- Batched reconstruction of many series (no counterpart in the reference,
