@@ -88,6 +88,10 @@ def lib():
             "or_wbp_rows32": (i, [P, P, P, i, i, i]),
             "or_wbp_rows64g": (i, [P, P, P, i, i, i]),
             "or_studio_reconstruct32": (None, [P, i, i, i, P, i, P]),
+            "or_ctf_wavelength": (d, [f]),
+            "or_ctf_strip_width": (i, [P, i, P, i]),
+            "or_ctfphaseflip32": (i, [P, P, i, i, i, P, i, P, i, P, P]),
+            "or_ctf_correct_strip32": (None, [P, P, P]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(_lib, name)
@@ -290,3 +294,54 @@ def studio_reconstruct(proj: np.ndarray, angles) -> np.ndarray:
     out = np.zeros((ny, nx, nx), np.float32)
     lib().or_studio_reconstruct32(_ptr(p), nx, ny, nz, _ptr(a), len(a), _ptr(out))
     return out
+
+
+class CtfParams(C.Structure):
+    """ctfphaseflip's options (apps/ctfphaseflip/src/main.rs:19-88 defaults)."""
+    _fields_ = [("defocus", C.c_float), ("voltage", C.c_float), ("cs", C.c_float), ("pixel_a", C.c_float),
+                ("strip_width", C.c_int32), ("tilt_axis_angle", C.c_float), ("max_strip_width", C.c_int32),
+                ("amplitude_contrast", C.c_float), ("cuton_freq", C.c_float), ("plate_phase", C.c_float)]
+
+    def __init__(self, **kw):
+        d = dict(defocus=-3000.0, voltage=300.0, cs=2.7, pixel_a=1.0, strip_width=256, tilt_axis_angle=0.0,
+                 max_strip_width=0, amplitude_contrast=0.07, cuton_freq=0.0, plate_phase=0.0)
+        d.update(kw)
+        super().__init__(**d)
+
+
+class CtfStrip(C.Structure):
+    """The shader's Params of apps/ctfphaseflip/src/ctf_correct.wgsl."""
+    _fields_ = [("sw", C.c_uint32), ("sh", C.c_uint32), ("pixel_a", C.c_float), ("wavelength", C.c_float),
+                ("cs_a", C.c_float), ("amp_contrast", C.c_float), ("cuton_freq", C.c_float),
+                ("defocus1", C.c_float), ("defocus2", C.c_float), ("astig_angle_rad", C.c_float),
+                ("has_astigmatism", C.c_uint32), ("plate_phase_rad", C.c_float), ("tilt_axis_rad", C.c_float)]
+
+
+def ctf_wavelength(kv):
+    return lib().or_ctf_wavelength(kv)
+
+
+def ctf_strip_width(params: CtfParams, nx, view_def=None):
+    vd = None if view_def is None else np.ascontiguousarray(view_def, dtype=np.float32).reshape(-1, 3)
+    return lib().or_ctf_strip_width(C.byref(params), nx, _ptr(vd), 0 if vd is None else len(vd))
+
+
+def ctfphaseflip(params: CtfParams, stack: np.ndarray, angles, view_def=None):
+    """ctfphaseflip of a [nz][ny][nx] stack (main.rs:231-700).  Returns (out, stats)."""
+    st_in = np.ascontiguousarray(stack, dtype=np.float32)
+    nz, ny, nx = st_in.shape
+    a = np.ascontiguousarray(angles, dtype=np.float32)
+    vd = None if view_def is None else np.ascontiguousarray(view_def, dtype=np.float32).reshape(-1, 3)
+    out = np.empty_like(st_in)
+    st = OrStats()
+    lib().or_ctfphaseflip32(C.byref(params), _ptr(st_in), nx, ny, nz, _ptr(a), len(a), _ptr(vd),
+                            0 if vd is None else len(vd), _ptr(out), C.byref(st))
+    return out, {"amin": st.amin, "amax": st.amax, "amean": st.amean}
+
+
+def ctf_correct_strip(re, im, strip: CtfStrip):
+    """ctf_correct.wgsl in f32 on one strip's re/im (copies returned)."""
+    r = np.array(re, dtype=np.float32, copy=True, order="C")
+    i = np.array(im, dtype=np.float32, copy=True, order="C")
+    lib().or_ctf_correct_strip32(_ptr(r), _ptr(i), C.byref(strip))
+    return r, i

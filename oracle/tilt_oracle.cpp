@@ -16,6 +16,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -764,3 +765,20 @@ void or_studio_reconstruct32(const float *proj, int nx, int ny, int nz, const fl
 }
 
 }  // extern "C"
+
+// f32 transform of any length for the ctfphaseflip restatement (ctf_oracle.cpp),
+// plans cached per length and thread
+namespace ctf_detail {
+void fft32(std::complex<float> *x, int n, bool inverse) {
+  thread_local std::vector<std::unique_ptr<FftPlan<float>>> plans;
+  thread_local std::vector<std::complex<float>> scratch;
+  FftPlan<float> *pl = nullptr;
+  for (auto &q : plans)
+    if (q->n == n) pl = q.get();
+  if (!pl) {
+    plans.emplace_back(new FftPlan<float>(n));
+    pl = plans.back().get();
+  }
+  pl->run(x, inverse, scratch);
+}
+}  // namespace ctf_detail

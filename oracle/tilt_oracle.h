@@ -114,6 +114,31 @@ int or_wbp_rows32(const or_params *p, const float *proj, float *vol_rows, int y0
 int or_wbp_rows64g(const or_params *p, const float *proj, double *vol_rows, int y0, int y1,
                    int nthreads);
 
+/* ---- ctfphaseflip (apps/ctfphaseflip/src/main.rs, ctf_correct.wgsl) ---- */
+typedef struct {
+  float defocus;             /* -d, nm (used without per-view values) */
+  float voltage;             /* kV */
+  float cs;                  /* mm */
+  float pixel_a;             /* pixel size, Angstrom */
+  int32_t strip_width;       /* -w */
+  float tilt_axis_angle;     /* degrees */
+  int32_t max_strip_width;   /* <= 0: automatic */
+  float amplitude_contrast;
+  float cuton_freq;          /* 1/Angstrom */
+  float plate_phase;         /* degrees */
+} or_ctf_params;
+typedef struct {             /* the shader's Params (ctf_correct.wgsl) */
+  uint32_t sw, sh;
+  float pixel_a, wavelength, cs_a, amp_contrast, cuton_freq, defocus1, defocus2, astig_angle_rad;
+  uint32_t has_astigmatism;
+  float plate_phase_rad, tilt_axis_rad;
+} or_ctf_strip;
+double or_ctf_wavelength(float kv);
+int or_ctf_strip_width(const or_ctf_params *p, int nx, const float *view_def, int nviews);
+int or_ctfphaseflip32(const or_ctf_params *p, const float *in, int nx, int ny, int nz, const float *angles,
+                      int n_angles, const float *view_def, int n_view_def, float *out, or_stats *st);
+void or_ctf_correct_strip32(float *re, float *im, const or_ctf_strip *p);
+
 /* imod-studio's reconstruction step (apps/imod-studio/src/main.rs:725-776) restated
  * directly: out[ny][nx][nx]. */
 void or_studio_reconstruct32(const float *proj, int nx, int ny, int nz, const float *angles,
