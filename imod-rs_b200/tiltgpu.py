@@ -63,6 +63,19 @@ class PhantomSpec(C.Structure):
                 ("noise_kind", _i32), ("noise", _f), ("xtilt_deg", _f)]
 
 
+class CtfOptions(C.Structure):
+    _fields_ = [("defocus", _f), ("voltage", _f), ("cs", _f), ("pixel_size", _f), ("strip_width", _i32),
+                ("tilt_axis_angle", _f), ("max_strip_width", _i32), ("amplitude_contrast", _f),
+                ("cuton_freq", _f), ("plate_phase", _f), ("device", _i32)]
+
+
+class CtfStripParams(C.Structure):
+    _fields_ = [("sw", C.c_uint32), ("sh", C.c_uint32), ("pixel_a", _f), ("wavelength", _f), ("cs_a", _f),
+                ("amp_contrast", _f), ("cuton_freq", _f), ("defocus1", _f), ("defocus2", _f),
+                ("astig_angle_rad", _f), ("has_astigmatism", C.c_uint32), ("plate_phase_rad", _f),
+                ("tilt_axis_rad", _f)]
+
+
 class MrcInfo(C.Structure):
     _fields_ = [("nx", _i32), ("ny", _i32), ("nz", _i32), ("mode", _i32), ("next", _i32),
                 ("swapped", _i32), ("xlen", _f), ("ylen", _f), ("zlen", _f), ("amin", _f),
@@ -138,6 +151,11 @@ EXPORTS = {
     "tg_apply_rweighting_device_noalloc": (C.c_int, [_P, C.c_size_t, C.c_size_t, C.c_size_t, _f, _f,
                                                      _i32, _i32, _i32, _P]),
     "tg_studio_reconstruct": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, _i32]),
+    "tg_ctf_options_default": (None, [C.POINTER(CtfOptions)]),
+    "tg_ctf_strip_width": (C.c_int, [C.POINTER(CtfOptions), _i32, _P, _i32, C.POINTER(_i32)]),
+    "tg_ctf_phaseflip": (C.c_int, [C.POINTER(CtfOptions), _P, _i32, _i32, _i32, _P, _i32, _P, _i32, _P,
+                                   C.POINTER(Stats)]),
+    "tg_ctf_correct_strip": (C.c_int, [_P, _P, C.POINTER(CtfStripParams), _i32]),
     "tg_upload_sections": (C.c_int, [_P, _i32, _i32, _P]),
     "tg_session_inject_wait_fault": (C.c_int, [_P, _i32, C.c_uint32]),
     "tg_download_slices_f16_async": (C.c_int, [_P, _i32, _i32, _P]),
@@ -543,6 +561,46 @@ def studio_reconstruct(ali_path, tlt_path, rec_path, device=0):
     """imod-studio's reconstruction step (apps/imod-studio/src/main.rs:725-776) on the GPU."""
     check(lib().tg_studio_reconstruct(str(ali_path).encode(), str(tlt_path).encode(), str(rec_path).encode(),
                                       device))
+
+
+def ctf_options(**kw):
+    """tg_ctf_options with the reference's defaults (apps/ctfphaseflip/src/main.rs:19-88)."""
+    o = CtfOptions()
+    lib().tg_ctf_options_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def ctf_phaseflip(stack, angles, view_defocus=None, **kw):
+    """CTF phase flip of a [nz][ny][nx] stack on the GPU.  Returns (out, stats)."""
+    st_in = _f32(stack)
+    nz, ny, nx = st_in.shape
+    a = _f32(angles)
+    vd = None if view_defocus is None else _f32(np.asarray(view_defocus).reshape(-1, 3))
+    o = ctf_options(**kw)
+    out = np.empty_like(st_in)
+    st = Stats()
+    check(lib().tg_ctf_phaseflip(C.byref(o), _ptr(st_in), nx, ny, nz, _ptr(a), len(a), _ptr(vd),
+                                 0 if vd is None else len(vd), _ptr(out), C.byref(st)))
+    return out, {"amin": st.amin, "amax": st.amax, "amean": st.amean}
+
+
+def ctf_strip_width(nx, view_defocus=None, **kw):
+    vd = None if view_defocus is None else _f32(np.asarray(view_defocus).reshape(-1, 3))
+    o = ctf_options(**kw)
+    w = _i32()
+    check(lib().tg_ctf_strip_width(C.byref(o), nx, _ptr(vd), 0 if vd is None else len(vd), C.byref(w)))
+    return w.value
+
+
+def ctf_correct_strip(re, im, device=0, **params):
+    """GpuCtfSession::correct_strip on one strip's 2D FFT (re, im: sw*sh floats); copies returned."""
+    r = np.array(re, dtype=np.float32, copy=True, order="C")
+    i = np.array(im, dtype=np.float32, copy=True, order="C")
+    p = CtfStripParams(**params)
+    check(lib().tg_ctf_correct_strip(_ptr(r), _ptr(i), C.byref(p), device))
+    return r, i
 
 
 def synth_projections(angles, *, nx, ny, vol_nx=None, vol_nz, n_ell=300, rmin=3.0, rmax=40.0,

@@ -320,6 +320,52 @@ int tg_apply_rweighting_device_noalloc(float *dev_proj, size_t in_nx, size_t in_
 int tg_studio_reconstruct(const char *ali_path, const char *tlt_path, const char *rec_path,
                           int32_t device);
 
+/* ---- ctfphaseflip: CTF phase flip of a tilt series (the step before tilt) ----
+ * Options of apps/ctfphaseflip/src/main.rs:19-88 (defaults via
+ * tg_ctf_options_default).  pixel_size is the caller's resolved value (the
+ * reference takes -p or the header's xlen/mx). */
+typedef struct {
+  float defocus;             /* -d, nm, used when no per-view values are given (-3000) */
+  float voltage;             /* -v, kV (300) */
+  float cs;                  /* -c, mm (2.7) */
+  float pixel_size;          /* -p or header, Angstrom */
+  int32_t strip_width;       /* -w (256) */
+  float tilt_axis_angle;     /* --tilt-axis-angle, degrees (0) */
+  int32_t max_strip_width;   /* --max-strip-width, <= 0: automatic (main.rs:297-320) */
+  float amplitude_contrast;  /* --amplitude-contrast (0.07) */
+  float cuton_freq;          /* --cuton-freq, 1/Angstrom (0) */
+  float plate_phase;         /* --plate-phase, degrees (0) */
+  int32_t device;            /* CUDA device ordinal */
+} tg_ctf_options;
+void tg_ctf_options_default(tg_ctf_options *o);
+/* The strip width the correction uses: strip_width clamped to the given or
+ * automatic maximum (main.rs:284-324).  view_defocus as in tg_ctf_phaseflip. */
+int tg_ctf_strip_width(const tg_ctf_options *o, int32_t nx, const float *view_defocus,
+                       int32_t n_view_defocus, int32_t *out);
+/* Replaces the per-view loop of main() (apps/ctfphaseflip/src/main.rs:385-700):
+ * host_in and host_out are [nz][ny][nx] floats (MrcReader::read_slice_f32
+ * order); angles are the .tlt values (missing views: 0); view_defocus holds 3
+ * floats per view (defocus1 nm, defocus2 nm, astigmatism angle degrees) after
+ * the reference's interpolation of the defocus file, or NULL to use
+ * o->defocus.  Every strip's 2D FFT, CTF sign flip (the CPU path's f64 CTF),
+ * inverse and weighted blend run on the GPU; stats receives the header
+ * statistics of main.rs:681-693. */
+int tg_ctf_phaseflip(const tg_ctf_options *o, const float *host_in, int32_t nx, int32_t ny, int32_t nz,
+                     const float *angles, int32_t n_angles, const float *view_defocus,
+                     int32_t n_view_defocus, float *host_out, tg_stats *stats);
+/* The shader's parameters (CtfParams of apps/ctfphaseflip/src/gpu.rs:8-26). */
+typedef struct {
+  uint32_t sw, sh;
+  float pixel_a, wavelength, cs_a, amp_contrast, cuton_freq, defocus1, defocus2, astig_angle_rad;
+  uint32_t has_astigmatism;
+  float plate_phase_rad, tilt_axis_rad;
+} tg_ctf_strip_params;
+/* Replaces GpuCtfSession::correct_strip (apps/ctfphaseflip/src/gpu.rs:107-262,
+ * ctf_correct.wgsl): flips, in place, the real and imaginary parts (sw*sh
+ * floats each, host memory) of one strip's 2D FFT where the CTF is negative,
+ * in the shader's f32 arithmetic. */
+int tg_ctf_correct_strip(float *strip_re, float *strip_im, const tg_ctf_strip_params *p, int32_t device);
+
 /* ---- Synthetic seeded inputs (no counterpart in the reference; the
  * workload generator for tests and benchmarks) ----
  * Projects a seeded random ellipsoid phantom (n_ell ellipsoids with semi-axes
