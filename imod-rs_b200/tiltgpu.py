@@ -16,6 +16,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("TILTGPU_LIB") or os.path.join(_HERE, "lib", "libtiltgpu.so")
 CLI_PATH = os.path.join(_HERE, "bin", "tilt")
+CTF_CLI_PATH = os.path.join(_HERE, "bin", "ctfphaseflip")
 
 TG_OK = 0
 STATUS = {0: "ok", -1: "invalid argument", -2: "out of device memory", -3: "CUDA error",

@@ -76,3 +76,50 @@ def test_ctf_strip_seam_vs_shader_restatement():
         differ = np.count_nonzero(gr != wr)
         assert differ <= 1e-4 * gr.size, differ
         assert 0.2 < np.mean(gr != re) < 0.8
+
+
+def interpolate(entries, n):
+    """interpolate_defocus of main.rs:162-209 (f32 lerp between listed views)."""
+    out = [None] * n
+    for v, d in entries:
+        if v < n:
+            out[v] = [np.float32(x) for x in d]
+    has = [o is not None for o in out]
+    res = [list(o) if o is not None else [np.float32(0)] * 3 for o in out]
+    for v in range(n):
+        if has[v]:
+            continue
+        b = next((i for i in range(v - 1, -1, -1) if has[i]), None)
+        a = next((i for i in range(v + 1, n) if has[i]), None)
+        if b is not None and a is not None:
+            t = np.float32(v - b) / np.float32(a - b)
+            res[v] = [res[b][k] + t * (res[a][k] - res[b][k]) for k in range(3)]
+        elif b is not None:
+            res[v] = list(res[b])
+        elif a is not None:
+            res[v] = list(res[a])
+    return np.array(res, np.float32)
+
+
+def test_ctfphaseflip_cli_with_defocus_file(tmp_path):
+    import subprocess
+    nz, ny, nx = 5, 48, 80
+    st_in = stack(nz, ny, nx, seed=9)
+    src, tlt, out, df = tmp_path / "in.mrc", tmp_path / "in.tlt", tmp_path / "out.mrc", tmp_path / "def.txt"
+    h = bytearray(T.mrc_header_new(nx, ny, nz, "Float"))
+    # xlen / mx = 2.5 A per pixel (the header's pixel size)
+    np.frombuffer(h, "<f4", 3, 40)[:] = (2.5 * nx, 2.5 * ny, 2.5 * nz)
+    T.mrc_write_f32(src, bytes(h), st_in)
+    ang = np.array([-40.0, -20.0, 0.0, 20.0, 40.0], np.float32)
+    T.write_tilt_file(tlt, ang)
+    df.write_text("# view def1 def2 astig\n0 -2000 -2400 30\n\n3 -3000\n")
+    r = subprocess.run([T.CTF_CLI_PATH, "-i", src, "-o", out, "-t", tlt, "--defocus-file", df, "-w", "32"],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    info, got = T.mrc_read(out)
+    assert (info.nx, info.ny, info.nz, info.mode) == (nx, ny, nz, 2)
+    assert b"ctfphaseflip: CTF phase correction (2D strips)" in bytes(info.header[224:304])
+    vd = interpolate([(0, (-2000, -2400, 30)), (3, (-3000, -3000, 0))], nz)
+    want, wst = O.ctfphaseflip(O.CtfParams(pixel_a=2.5, strip_width=32), st_in, T.read_tilt_file(tlt), vd)
+    assert rel_l2(got.reshape(want.shape), want) <= 1e-5
+    assert info.amean == pytest.approx(wst["amean"], rel=1e-5)
