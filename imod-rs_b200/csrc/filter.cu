@@ -413,13 +413,12 @@ __device__ __forceinline__ float2 *p2_fft(float2 (&x)[V], int t, const float2 *_
 }
 
 template <int N, int V, int FMT, int STORE>
-__global__ void __launch_bounds__(N / V) filter_p2_kernel(FilterArgs a) {
+__device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp, const int v) {
   extern __shared__ __align__(16) unsigned char fsm[];
   constexpr int T = N / V;
   float2 *A = reinterpret_cast<float2 *>(fsm);
   float2 *B = A + N;
   const int t = threadIdx.x;
-  const int jp = blockIdx.x, v = blockIdx.y;
   const int r0 = 2 * jp;
   const bool has1 = r0 + 1 < a.ny;
   const float *in0 = a.in + ((size_t)v * a.ny + r0) * N;
@@ -540,6 +539,37 @@ __global__ void __launch_bounds__(N / V) filter_p2_kernel(FilterArgs a) {
   range_report<STORE>(a, hmax);
 }
 
+template <int N, int V, int FMT, int STORE>
+__global__ void __launch_bounds__(N / V) filter_p2_kernel(FilterArgs a) {
+  filter_p2_body<N, V, FMT, STORE>(a, blockIdx.x, blockIdx.y);
+}
+
+// The same filter over the row pairs of many series of one width: block b
+// belongs to series j with blk0[j] <= b < blk0[j+1] ((ny+1)/2 row pairs x views
+// each); every series' rows come out as in its own launch.
+template <int N, int V, int FMT, int STORE>
+__global__ void __launch_bounds__(N / V) filter_p2_batch_kernel(FilterBatchDev fb) {
+  __shared__ __align__(16) FilterArgs s_a;
+  __shared__ int s_j;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = fb.njobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(&fb.blk0[mid]) <= (int)blockIdx.x) lo = mid;
+      else hi = mid - 1;
+    }
+    s_j = lo;
+  }
+  __syncthreads();
+  const int j = s_j;
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(&fb.jobs[j]);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(&s_a);
+  for (int i = threadIdx.x; i < (int)(sizeof(FilterArgs) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  const int t = (int)blockIdx.x - __ldg(&fb.blk0[j]), nrp = (s_a.ny + 1) / 2;
+  filter_p2_body<N, V, FMT, STORE>(s_a, t % nrp, t / nrp);
+}
+
 template <int N, int V, int FMT, int STORE> static void launch_p2(const FilterArgs &a, cudaStream_t st) {
   const size_t smem = (size_t)N * 16;
   auto k = filter_p2_kernel<N, V, FMT, STORE>;
@@ -569,6 +599,48 @@ template <int FMT, int STORE> static void launch_f(const FilterArgs &a, cudaStre
   auto k = filter_kernel<FMT, STORE>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k<<<dim3((a.ny + 1) / 2, a.nviews), 256, smem, st>>>(a);
+}
+
+int filter_batch_width(const FilterArgs &a) {
+  if (!a.weights || a.conv_h || getenv("TG_FILTER_GENERIC")) return 0;
+  switch (a.nx) {
+    case 256: case 512: case 1024: case 2048: case 4096: case 384: case 768: case 1536: case 3072: return a.nx;
+    default: return 0;
+  }
+}
+
+template <int N, int V, int FMT, int STORE>
+static void launch_p2_batch(const FilterBatchDev &fb, int nblocks, cudaStream_t st) {
+  const size_t smem = (size_t)N * 16;
+  auto k = filter_p2_batch_kernel<N, V, FMT, STORE>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k<<<nblocks, N / V, smem, st>>>(fb);
+}
+
+template <int FMT, int STORE> static void launch_batch_n(int n, const FilterBatchDev &fb, int nb, cudaStream_t st) {
+  switch (n) {
+    case 256: launch_p2_batch<256, 8, FMT, STORE>(fb, nb, st); break;
+    case 512: launch_p2_batch<512, 8, FMT, STORE>(fb, nb, st); break;
+    case 1024: launch_p2_batch<1024, 8, FMT, STORE>(fb, nb, st); break;
+    case 2048: launch_p2_batch<2048, 8, FMT, STORE>(fb, nb, st); break;
+    case 4096: launch_p2_batch<4096, 8, FMT, STORE>(fb, nb, st); break;
+    case 384: launch_p2_batch<384, 12, FMT, STORE>(fb, nb, st); break;
+    case 768: launch_p2_batch<768, 24, FMT, STORE>(fb, nb, st); break;
+    case 1536: launch_p2_batch<1536, 24, FMT, STORE>(fb, nb, st); break;
+    default: launch_p2_batch<3072, 24, FMT, STORE>(fb, nb, st); break;
+  }
+}
+
+void launch_filter_batch(int n, int fmt, int store, const FilterBatchDev &fb, int nblocks, cudaStream_t st) {
+  if (fmt == FMT_ROWPAIR) {
+    if (store == TG_STORE_FP32) launch_batch_n<FMT_ROWPAIR, TG_STORE_FP32>(n, fb, nblocks, st);
+    else if (store == TG_STORE_FP16) launch_batch_n<FMT_ROWPAIR, TG_STORE_FP16>(n, fb, nblocks, st);
+    else launch_batch_n<FMT_ROWPAIR, TG_STORE_BF16>(n, fb, nblocks, st);
+  } else {
+    if (store == TG_STORE_FP32) launch_batch_n<FMT_SINGLE, TG_STORE_FP32>(n, fb, nblocks, st);
+    else if (store == TG_STORE_FP16) launch_batch_n<FMT_SINGLE, TG_STORE_FP16>(n, fb, nblocks, st);
+    else launch_batch_n<FMT_SINGLE, TG_STORE_BF16>(n, fb, nblocks, st);
+  }
 }
 
 void launch_filter(const FilterArgs &a, cudaStream_t st) {

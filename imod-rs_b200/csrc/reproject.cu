@@ -128,10 +128,10 @@ __global__ void __launch_bounds__(128) fp_kernel(FpArgs a) {
 // Grid: (views, bin blocks, row groups) -- the views of one row group run
 // together, so their reads of that slab of the volume hit L2.
 template <int S, bool XT, bool IL>
-__global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
-  const int v = blockIdx.x;
-  const int p = blockIdx.y * blockDim.x + threadIdx.x;
-  const int r0 = blockIdx.z * S;
+__device__ __forceinline__ void fp_fast_body(const FpArgs &a, const int bx, const int by, const int bz) {
+  const int v = bx;
+  const int p = by * blockDim.x + threadIdx.x;
+  const int r0 = bz * S;
   if (p >= a.nx) return;
   const int nrows = min(S, a.ny - r0);
   if (v >= a.nviews) {  // views without a tilt angle contribute nothing (main.rs:683-686)
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
         // per 4-row plane (neighbouring threads' columns are neighbouring float4s); with
         // x-tilt each holds the row's blend of its two source slices (blend_interleave_kernel)
         const float4 *q = reinterpret_cast<const float4 *>(a.volg) +
-                          ((size_t)blockIdx.z * a.onz + oz) * a.onx * (S / 4) + ox;
+                          ((size_t)bz * a.onz + oz) * a.onx * (S / 4) + ox;
         // products on the f32x2 pipe; the sums stay scalar so that no product is
         // contracted into them (each stays RN(acc + RN(v*w)), the reference's operations)
         const uint64_t w2 = pk2(w, w);
@@ -258,9 +258,8 @@ __global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
 // volg[g][oz][j/4][ox][j%4] = vol[g*G + j][oz][ox] (zero for rows past ny): per
 // (row group, depth) G/4 planes of float4s, each plane a row of columns
 template <int G>
-__global__ void interleave_kernel(const float *__restrict__ vol, float *__restrict__ volg, int ny,
+__device__ __forceinline__ void interleave_at(size_t i, const float *__restrict__ vol, float *__restrict__ volg, int ny,
                                   int onz, int onx, size_t n) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (g, oz, ox)
   if (i >= n) return;
   const size_t sl = (size_t)onz * onx;
   const size_t g = i / sl, rem = i - g * sl;
@@ -275,6 +274,11 @@ __global__ void interleave_kernel(const float *__restrict__ vol, float *__restri
 #pragma unroll
   for (int k = 0; k < G / 4; ++k)
     o[(size_t)k * onx] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+}
+
+template <int G>
+__global__ void interleave_kernel(const float *__restrict__ vol, float *__restrict__ volg, int ny, int onz, int onx, size_t n) {
+  interleave_at<G>((size_t)blockIdx.x * blockDim.x + threadIdx.x, vol, volg, ny, onz, onx, n);
 }
 
 // ---- half-precision reprojection (FP16/BF16 staging forms) ----
@@ -308,11 +312,13 @@ __device__ __forceinline__ float half_scale(const unsigned *maxbits, bool invers
   return inverse ? ldexpf(1.0f, e - 9) : ldexpf(1.0f, 9 - e);
 }
 
-__global__ void absmax_kernel(const float *__restrict__ vol, size_t n, unsigned *maxbits) {
+// block blk of nblk blocks folds its share of max|vol| into *maxbits
+__device__ __forceinline__ void absmax_at(const float *__restrict__ vol, size_t n, unsigned *maxbits, int blk,
+                                          int nblk) {
   float m = 0.0f;
-  const size_t n4 = n / 4, stride = (size_t)gridDim.x * blockDim.x;
+  const size_t n4 = n / 4, stride = (size_t)nblk * blockDim.x;
   const float4 *v4 = reinterpret_cast<const float4 *>(vol);  // cudaMalloc'd: 16-byte aligned
-  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t i = (size_t)blk * blockDim.x + threadIdx.x;
   for (; i + 3 * stride < n4; i += 4 * stride) {  // four independent 16-byte loads in flight
     const float4 a = __ldg(v4 + i), b = __ldg(v4 + i + stride), c = __ldg(v4 + i + 2 * stride),
                  d = __ldg(v4 + i + 3 * stride);
@@ -325,16 +331,19 @@ __global__ void absmax_kernel(const float *__restrict__ vol, size_t n, unsigned 
     const float4 a = __ldg(v4 + i);
     m = fmaxf(m, fmaxf(fmaxf(fabsf(a.x), fabsf(a.y)), fmaxf(fabsf(a.z), fabsf(a.w))));
   }
-  if (blockIdx.x == 0 && threadIdx.x < n - 4 * n4) m = fmaxf(m, fabsf(__ldg(vol + 4 * n4 + threadIdx.x)));
+  if (blk == 0 && threadIdx.x < n - 4 * n4) m = fmaxf(m, fabsf(__ldg(vol + 4 * n4 + threadIdx.x)));
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(maxbits, __float_as_uint(m));  // |v| orders as its bits
 }
 
+__global__ void absmax_kernel(const float *__restrict__ vol, size_t n, unsigned *maxbits) {
+  absmax_at(vol, n, maxbits, blockIdx.x, gridDim.x);
+}
+
 // volh[g][oz][j/8][ox][j%8] = half(vol[g*G + j][oz][ox] * scale) (zero past ny)
 template <int G>
-__global__ void interleave_half_kernel(const float *__restrict__ vol, __half *__restrict__ volh, int ny,
+__device__ __forceinline__ void interleave_half_at(size_t i, const float *__restrict__ vol, __half *__restrict__ volh, int ny,
                                        int onz, int onx, size_t n, const unsigned *maxbits) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (g, oz, ox)
   if (i >= n) return;
   const float sc = half_scale(maxbits, false);
   const size_t sl = (size_t)onz * onx;
@@ -355,11 +364,17 @@ __global__ void interleave_half_kernel(const float *__restrict__ vol, __half *__
     o[(size_t)k * onx] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
 }
 
+template <int G>
+__global__ void interleave_half_kernel(const float *__restrict__ vol, __half *__restrict__ volh, int ny, int onz, int onx, size_t n,
+                                       const unsigned *maxbits) {
+  interleave_half_at<G>((size_t)blockIdx.x * blockDim.x + threadIdx.x, vol, volh, ny, onz, onx, n, maxbits);
+}
+
 template <int S, bool XT>
-__global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
-  const int v = blockIdx.x;
-  const int p = blockIdx.y * blockDim.x + threadIdx.x;
-  const int r0 = blockIdx.z * S;
+__device__ __forceinline__ void fp_half_body(const FpArgs &a, const int bx, const int by, const int bz) {
+  const int v = bx;
+  const int p = by * blockDim.x + threadIdx.x;
+  const int r0 = bz * S;
   if (p >= a.nx) return;
   const int nrows = min(S, a.ny - r0);
   if (v >= a.nviews) {  // views without a tilt angle contribute nothing (main.rs:683-686)
@@ -383,7 +398,7 @@ __global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
   const float c = XT ? cos_t * cos_xt : cos_t;
   float c0 = 0.0f;
   auto X = [&](float fo) { return fmaf(fo, c, c0); };  // fo: the column as a float
-  const uint4 *vg = reinterpret_cast<const uint4 *>(a.volh) + (size_t)blockIdx.z * a.onz * a.onx * (S / 8);
+  const uint4 *vg = reinterpret_cast<const uint4 *>(a.volh) + (size_t)bz * a.onz * a.onx * (S / 8);
   float foz = 0.0f;
   for (int oz = 0; oz < a.onz; ++oz, foz += 1.0f) {
     const float dz = __fsub_rn(foz, a.cz);
@@ -462,9 +477,8 @@ __device__ __forceinline__ float blend_row(const float *__restrict__ vol, int ny
 }
 
 template <int G>
-__global__ void blend_interleave_kernel(const float *__restrict__ vol, float *__restrict__ volb, int ny,
+__device__ __forceinline__ void blend_interleave_at(size_t i, const float *__restrict__ vol, float *__restrict__ volb, int ny,
                                         int onz, int onx, float ocx, float sin_xt, size_t n) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (g, oz, ox)
   if (i >= n) return;
   const size_t sl = (size_t)onz * onx;
   const size_t g = i / sl, rem = i - g * sl;
@@ -481,13 +495,18 @@ __global__ void blend_interleave_kernel(const float *__restrict__ vol, float *__
     o[(size_t)k * onx] = make_float4(b[4 * k], b[4 * k + 1], b[4 * k + 2], b[4 * k + 3]);
 }
 
+template <int G>
+__global__ void blend_interleave_kernel(const float *__restrict__ vol, float *__restrict__ volb, int ny, int onz, int onx,
+                                        float ocx, float sin_xt, size_t n) {
+  blend_interleave_at<G>((size_t)blockIdx.x * blockDim.x + threadIdx.x, vol, volb, ny, onz, onx, ocx, sin_xt, n);
+}
+
 // The same blend into the scaled FP16 copy of the half-staging forms (a blend of
 // two slices is below 2 max|v|: one more bit of headroom).
 template <int G>
-__global__ void blend_interleave_half_kernel(const float *__restrict__ vol, __half *__restrict__ volh, int ny,
+__device__ __forceinline__ void blend_interleave_half_at(size_t i, const float *__restrict__ vol, __half *__restrict__ volh, int ny,
                                              int onz, int onx, float ocx, float sin_xt, size_t n,
                                              const unsigned *maxbits) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // (g, oz, ox)
   if (i >= n) return;
   const float sc = half_scale(maxbits, false, 1);
   const size_t sl = (size_t)onz * onx;
@@ -508,6 +527,89 @@ __global__ void blend_interleave_half_kernel(const float *__restrict__ vol, __ha
 #pragma unroll
   for (int k = 0; k < G / 8; ++k)
     o[(size_t)k * onx] = make_uint4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
+}
+
+template <int G>
+__global__ void blend_interleave_half_kernel(const float *__restrict__ vol, __half *__restrict__ volh, int ny, int onz,
+                                             int onx, float ocx, float sin_xt, size_t n, const unsigned *maxbits) {
+  blend_interleave_half_at<G>((size_t)blockIdx.x * blockDim.x + threadIdx.x, vol, volh, ny, onz, onx, ocx, sin_xt, n, maxbits);
+}
+
+template <int S, bool XT, bool IL>
+__global__ void __launch_bounds__(128) fp_fast_kernel(FpArgs a) {
+  fp_fast_body<S, XT, IL>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <int S, bool XT>
+__global__ void __launch_bounds__(128) fp_half_kernel(FpArgs a) {
+  fp_half_body<S, XT>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// ---- batched reprojection: one launch per phase over the blocks of many series ----
+// Block b belongs to series j with blk0[j] <= b < blk0[j+1]; its arguments are
+// copied to shared memory and the per-series body runs with the block's local
+// coordinates, so every series' result is the same as in its own launch.
+__device__ __forceinline__ int load_fp_job(const FpBatchDev &b, FpArgs *s_a) {
+  __shared__ int s_j;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = b.njobs - 1;  // last series whose first block is <= blockIdx.x
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(&b.blk0[mid]) <= (int)blockIdx.x) lo = mid;
+      else hi = mid - 1;
+    }
+    s_j = lo;
+  }
+  __syncthreads();
+  const int j = s_j;
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(&b.jobs[j]);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(s_a);
+  for (int i = threadIdx.x; i < (int)(sizeof(FpArgs) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  return (int)blockIdx.x - __ldg(&b.blk0[j]);
+}
+
+__global__ void fp_zero_maxbits_kernel(const FpArgs *jobs, int njobs) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < njobs) *jobs[j].maxbits = 0u;
+}
+
+__global__ void __launch_bounds__(256) absmax_batch_kernel(FpBatchDev b) {
+  __shared__ __align__(16) FpArgs s_a;
+  const int t = load_fp_job(b, &s_a);
+  const size_t n = (size_t)s_a.ny * s_a.onz * s_a.onx;
+  absmax_at(s_a.vol, n, s_a.maxbits, t, fp_absmax_blocks(n));
+}
+
+template <int S, bool HALF, bool XT>
+__global__ void __launch_bounds__(256) fp_copy_batch_kernel(FpBatchDev b) {
+  __shared__ __align__(16) FpArgs s_a;
+  const int t = load_fp_job(b, &s_a);
+  const FpArgs &a = s_a;
+  const size_t n = (size_t)((a.ny + S - 1) / S) * a.onz * a.onx;
+  const size_t i = (size_t)t * 256 + threadIdx.x;
+  if (HALF) {
+    if (XT) blend_interleave_half_at<S>(i, a.vol, (__half *)a.volh, a.ny, a.onz, a.onx, a.ocx, a.sin_xt_common, n, a.maxbits);
+    else interleave_half_at<S>(i, a.vol, (__half *)a.volh, a.ny, a.onz, a.onx, n, a.maxbits);
+  } else {
+    if (XT) blend_interleave_at<S>(i, a.vol, a.volg, a.ny, a.onz, a.onx, a.ocx, a.sin_xt_common, n);
+    else interleave_at<S>(i, a.vol, a.volg, a.ny, a.onz, a.onx, n);
+  }
+}
+
+template <int S, bool XT, bool IL>
+__global__ void __launch_bounds__(128) fp_fast_batch_kernel(FpBatchDev b) {
+  __shared__ __align__(16) FpArgs s_a;
+  const int t = load_fp_job(b, &s_a);
+  const int gx = s_a.nviews_all, gy = (s_a.nx + 127) / 128;
+  fp_fast_body<S, XT, IL>(s_a, t % gx, (t / gx) % gy, t / (gx * gy));
+}
+
+template <int S, bool XT>
+__global__ void __launch_bounds__(128) fp_half_batch_kernel(FpBatchDev b) {
+  __shared__ __align__(16) FpArgs s_a;
+  const int t = load_fp_job(b, &s_a);
+  const int gx = s_a.nviews_all, gy = (s_a.nx + 127) / 128;
+  fp_half_body<S, XT>(s_a, t % gx, (t / gx) % gy, t / (gx * gy));
 }
 
 template <int S>
@@ -552,6 +654,63 @@ static int launch_fast(const FpArgs &a, cudaStream_t st) {
 }
 
 int fp_group_rows(int variant) { return variant == 1 || variant == 3 ? 16 : 8; }
+
+// key = form * 1000 + rows per thread * 10 + x-tilt * 2 + interleaved copy
+// (form 1: scaled FP16 copy, 2: FP32 fast kernel)
+int fp_batch_key(const FpArgs &a) {
+  if ((a.fast == 1 || a.fast == 2) && a.volh) return 1000 + fp_half_rows(a.variant) * 10 + (a.fast == 2 ? 2 : 0) + 1;
+  if (a.fast == 1 || a.fast == 2) return 2000 + fp_group_rows(a.variant) * 10 + (a.fast == 2 ? 2 : 0) + (a.volg ? 1 : 0);
+  return -1;
+}
+
+void fp_batch_blocks(const FpArgs &a, int key, int *absmax, int *copy, int *fp) {
+  const int S = (key % 1000) / 10;
+  const bool half = key / 1000 == 1, il = (key & 1) != 0;
+  const size_t n = (size_t)((a.ny + S - 1) / S) * a.onz * a.onx;
+  *absmax = half ? fp_absmax_blocks((size_t)a.ny * a.onz * a.onx) : 0;
+  *copy = (half || il) ? (int)((n + 255) / 256) : 0;
+  *fp = a.nviews_all * ((a.nx + 127) / 128) * ((a.ny + S - 1) / S);
+}
+
+template <int S, bool HALF, bool XT, bool IL>
+static int launch_batch_t(const FpArgs *jobs, int njobs, const int *blk_abs, int nabs, const int *blk_copy,
+                          int ncopy, const int *blk_fp, int nfp, cudaStream_t st) {
+  int k = 0;
+  if (HALF) {
+    fp_zero_maxbits_kernel<<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs);
+    absmax_batch_kernel<<<nabs, 256, 0, st>>>(FpBatchDev{jobs, blk_abs, njobs});
+    k += 2;
+  }
+  if (HALF || IL) {
+    fp_copy_batch_kernel<S, HALF, XT><<<ncopy, 256, 0, st>>>(FpBatchDev{jobs, blk_copy, njobs});
+    ++k;
+  }
+  if (HALF) fp_half_batch_kernel<S, XT><<<nfp, 128, 0, st>>>(FpBatchDev{jobs, blk_fp, njobs});
+  else fp_fast_batch_kernel<S, XT, IL><<<nfp, 128, 0, st>>>(FpBatchDev{jobs, blk_fp, njobs});
+  return k + 1;
+}
+
+int launch_reproject_batch(int key, const FpArgs *jobs, int njobs, const int *blk_abs, int nabs,
+                           const int *blk_copy, int ncopy, const int *blk_fp, int nfp, cudaStream_t st) {
+#define TG_FPB(KEY, S, HALF, XT, IL) \
+  case KEY: return launch_batch_t<S, HALF, XT, IL>(jobs, njobs, blk_abs, nabs, blk_copy, ncopy, blk_fp, nfp, st);
+  switch (key) {
+    TG_FPB(1161, 16, true, false, true)
+    TG_FPB(1163, 16, true, true, true)
+    TG_FPB(1321, 32, true, false, true)
+    TG_FPB(1323, 32, true, true, true)
+    TG_FPB(2080, 8, false, false, false)
+    TG_FPB(2081, 8, false, false, true)
+    TG_FPB(2082, 8, false, true, false)
+    TG_FPB(2083, 8, false, true, true)
+    TG_FPB(2160, 16, false, false, false)
+    TG_FPB(2161, 16, false, false, true)
+    TG_FPB(2162, 16, false, true, false)
+    TG_FPB(2163, 16, false, true, true)
+    default: return 0;
+  }
+#undef TG_FPB
+}
 
 // ---- local alignment ----
 // The table of corrections: ViewPatches::interpolate (main.rs:172-228) at every

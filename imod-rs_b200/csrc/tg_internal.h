@@ -66,6 +66,15 @@ struct FilterArgs {
   int *err;                 // session error word: bit 2 set when a value exceeds the FP16 range
 };
 void launch_filter(const FilterArgs &a, cudaStream_t st);
+// ---- the register-resident filter over many series of one width in one launch ----
+struct FilterBatchDev {
+  const FilterArgs *jobs;   // device array
+  const int *blk0;          // njobs + 1 prefix sums of ((ny + 1) / 2) * nviews blocks
+  int njobs;
+};
+// the row width a series' filter shares launches by, or 0 when it runs on its own
+int filter_batch_width(const FilterArgs &a);
+void launch_filter_batch(int n, int fmt, int store, const FilterBatchDev &fb, int nblocks, cudaStream_t st);
 // radial weight table of apps/tilt/src/main.rs:348-369 in f32 (host)
 void weight_table(int n, float cutoff, float falloff, int efs, int hamming, float *wt);
 
@@ -171,6 +180,26 @@ void launch_local_table(const LocalDev &L, int nviews, int ny, int onx, float2 *
 void launch_local_bounds(const float2 *table, int nviews, int ny, int onx, float2 *bnd, cudaStream_t st);
 int fp_group_rows(int variant);
 int fp_half_rows(int variant);
+// ---- batched reprojection (one launch per phase over the series of a group) ----
+struct FpBatchDev {
+  const FpArgs *jobs;       // device array of per-series arguments
+  const int *blk0;          // njobs + 1 prefix sums of the phase's blocks per series
+  int njobs;
+};
+// blocks of the max|vol| pass of a volume of n values (one series)
+inline __host__ __device__ int fp_absmax_blocks(size_t n) {
+  const size_t b = (n + 4095) / 4096;
+  return (int)(b < 1 ? 1 : b > 1184 ? 1184 : b);
+}
+// the batched form a series' reprojection takes (series with equal keys share
+// launches), or -1 when it is launched on its own (local alignment, general kernel)
+int fp_batch_key(const FpArgs &a);
+// blocks of each phase of one series in its group: max|vol|, copy, projection
+void fp_batch_blocks(const FpArgs &a, int key, int *absmax, int *copy, int *fp);
+// the phases of one group; jobs and the three prefix arrays in device memory,
+// totals = the last prefix entries.  Returns the kernels launched.
+int launch_reproject_batch(int key, const FpArgs *jobs, int njobs, const int *blk_abs, int nabs,
+                           const int *blk_copy, int ncopy, const int *blk_fp, int nfp, cudaStream_t st);
 
 // ---- volume operations ----
 void launch_lowpass(float *vol, float *tmp, int onx, int onz, int ny, cudaStream_t st);
