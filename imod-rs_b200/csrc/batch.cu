@@ -110,12 +110,14 @@ int tg_batch_add(tg_batch *b, tg_session *s) {
   if (s->dev != b->dev) { set_error("session and batch are on different devices"); return TG_ERR_INVALID_ARG; }
   if (std::find(b->sess.begin(), b->sess.end(), s) != b->sess.end()) return TG_OK;
   b->sess.push_back(s);
+  ++b->generation;
   return TG_OK;
 }
 
 int tg_batch_clear(tg_batch *b) {
   if (!b) return TG_ERR_INVALID_ARG;
   b->sess.clear();
+  ++b->generation;
   return TG_OK;
 }
 
@@ -149,19 +151,28 @@ int tg_batch_reconstruct(tg_batch *b) {
   if ((rc = batch_bp(b, b->sess, modes, nt0, &launches)) != TG_OK) { restore(); return rc; }
   int max_it = 0;
   for (tg_session *s : b->sess) max_it = std::max(max_it, sirt_iters(s));
-  // round r: the r-th SIRT update of every series that still iterates
+  // round r: the r-th SIRT update of every series that still iterates, as one
+  // plan of grouped launches (round.cu); rounds with the same members replay the
+  // plan's CUDA graph
+  b->graph_launches = 0;
   for (int r = 1; r <= max_it; ++r) {
     NvtxRange nv("tg.batch.sirt_round");
     std::vector<tg_session *> act;
+    bool graphs = true;
     for (tg_session *s : b->sess)
       if (sirt_iters(s) >= r) {
-        launches += launch_reproject(fp_args(s), s->st);
-        launch_filter(filter_args(s, true), s->st);
-        launches += 1;
         act.push_back(s);
+        graphs &= s->o.use_graphs != 0;
       }
-    std::vector<int> m2(act.size(), 2);
-    if ((rc = batch_bp(b, act, m2, nt, &launches)) != TG_OK) { restore(); return rc; }
+    std::vector<uint64_t> key{b->generation, (uint64_t)act.size()};
+    for (tg_session *s : act) key.push_back((uint64_t)(uintptr_t)s);
+    round_plan_signature(act, key);
+    if (key != b->plan.key && (rc = round_plan_build(b->plan, act, key, b->st)) != TG_OK) { restore(); return rc; }
+    rc = graphs ? round_plan_launch_graph(b->plan, b->st) : round_plan_issue(b->plan, b->st);
+    if (rc != TG_OK) { restore(); return rc; }
+    if (graphs) ++b->graph_launches;
+    launches += b->plan.launches;
+    b->persistent_launches += (int)b->plan.bp.size();
   }
   double updates = 0.0;
   for (size_t i = 0; i < b->sess.size(); ++i) {
@@ -212,9 +223,23 @@ int tg_batch_last_run(tg_batch *b, tg_run_info *info) {
   return TG_OK;
 }
 
+// Plan of the last batched reconstruction's SIRT rounds (tests and profiling):
+// rounds replayed from a CUDA graph, grouped reprojection and filter launches,
+// kernels per round.
+int tg_batch_plan_info(tg_batch *b, int32_t *graph_rounds, int32_t *fp_groups, int32_t *filter_groups,
+                       int32_t *round_launches) {
+  if (!b) return TG_ERR_INVALID_ARG;
+  if (graph_rounds) *graph_rounds = b->graph_launches;
+  if (fp_groups) *fp_groups = (int32_t)b->plan.fp.size();
+  if (filter_groups) *filter_groups = (int32_t)b->plan.fi.size();
+  if (round_launches) *round_launches = b->plan.launches;
+  return TG_OK;
+}
+
 int tg_batch_destroy(tg_batch *b) {
   if (!b) return TG_ERR_INVALID_ARG;
   cudaSetDevice(b->dev);
+  round_plan_release(b->plan, b->st);
   cudaStreamSynchronize(b->st);
   cudaFree(b->d_jobs);
   cudaFree(b->d_counter);

@@ -86,6 +86,8 @@ struct tg_server {
   cudaStream_t cs = nullptr, us = nullptr, ds = nullptr, fs = nullptr;
   cudaMemPool_t pool = nullptr;
   tg_batch batch;
+  RoundPlan plan, scratch;    // SIRT rounds: the captured plan, and the plan of the last round
+  uint64_t graph_rounds = 0;  // device thread only
   unsigned char *h_slots = nullptr;
   std::vector<int> free_slots;                  // guarded by mu
   std::mutex ev_mu;                             // guards event_pool
@@ -350,8 +352,12 @@ bool run_round(tg_server *sv) {
   NvtxRange nv("tg.server.round");
   cudaEvent_t r0 = take_timing_event(sv);
   if (r0) cudaEventRecord(r0, sv->cs);
-  std::vector<tg_session *> ss;
+  // jobs in their first round: log/means, filter, one WBP back-projection launch;
+  // jobs in SIRT rounds: one plan of grouped launches (round.cu), replayed from its
+  // CUDA graph while the same jobs keep iterating together
+  std::vector<tg_session *> first, iter;
   std::vector<int> modes, nt;
+  std::vector<uint64_t> key;
   int launches = 0, rc = TG_OK;
   for (auto &j : ready) {
     tg_session *s = j->s;
@@ -359,15 +365,31 @@ bool run_round(tg_server *sv) {
       cudaStreamWaitEvent(sv->cs, j->ev_up, 0);
       if (rc == TG_OK) rc = stage_front(s, &launches);
       modes.push_back(first_mode(s));
+      first.push_back(s);
     } else {
-      launch_reproject(fp_args(s), sv->cs);
-      launch_filter(filter_args(s, true), sv->cs);
-      modes.push_back(2);
+      iter.push_back(s);
+      key.push_back(j->id);
     }
-    ss.push_back(s);
   }
   sv->batch.persistent_launches = 0;
-  if (rc == TG_OK) rc = batch_bp(&sv->batch, ss, modes, nt, &launches);
+  if (rc == TG_OK && !iter.empty()) {
+    round_plan_signature(iter, key);
+    if (key == sv->plan.key) {
+      rc = round_plan_launch_graph(sv->plan, sv->cs);
+      ++sv->graph_rounds;
+    } else if (key == sv->scratch.key) {  // the same jobs a second round in a row: capture
+      std::swap(sv->plan, sv->scratch);
+      rc = round_plan_launch_graph(sv->plan, sv->cs);
+      ++sv->graph_rounds;
+    } else {
+      rc = round_plan_build(sv->scratch, iter, key, sv->cs);
+      if (rc == TG_OK) rc = round_plan_issue(sv->scratch, sv->cs);
+    }
+    const RoundPlan &p = key == sv->plan.key ? sv->plan : sv->scratch;
+    launches += p.launches;
+    sv->batch.persistent_launches += (int)p.bp.size();
+  }
+  if (rc == TG_OK && !first.empty()) rc = batch_bp(&sv->batch, first, modes, nt, &launches);
   if (rc != TG_OK) {  // a launch could not be issued: the round's jobs fail, the others go on
     for (auto &j : ready) {
       drop_active(sv, j);
@@ -377,12 +399,13 @@ bool run_round(tg_server *sv) {
     if (r0) sv->timing_pool.push_back(r0);
     return true;
   }
-  for (size_t i = 0; i < ready.size(); ++i) {
+  for (size_t i = 0, fi = 0; i < ready.size(); ++i) {
     std::shared_ptr<SJob> j = ready[i];
     tg_session *s = j->s;
     if (j->rounds_done == 0) {
-      j->mode0 = modes[i];
-      j->nt0 = nt[i];
+      j->mode0 = modes[fi];
+      j->nt0 = nt[fi];
+      ++fi;
     }
     if (++j->rounds_done < j->rounds_total) continue;
     rc = stage_finish(s, j->mode0, j->nt0, &launches);
@@ -442,6 +465,8 @@ void device_loop(tg_server *sv) {
     collect(sv);
     if (!run_round(sv)) std::this_thread::sleep_for(std::chrono::microseconds(100));
   }
+  round_plan_release(sv->plan, sv->cs);
+  round_plan_release(sv->scratch, sv->cs);
   cudaStreamSynchronize(sv->cs);
   cudaStreamSynchronize(sv->us);
   cudaStreamSynchronize(sv->ds);

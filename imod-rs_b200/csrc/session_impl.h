@@ -1,6 +1,8 @@
 // session_impl.h -- the session object and the stage helpers shared by the
 // per-series C ABI (session.cu) and the batched launch (batch.cu).
 #pragma once
+#include <cstring>
+#include <tuple>
 #include <vector>
 
 #include "tg_internal.h"
@@ -104,6 +106,33 @@ int batch_bp(tg_batch *b, const std::vector<tg_session *> &ss, const std::vector
 
 }  // namespace tg
 
+namespace tg {
+// One SIRT round over many series: grouped launches from tables in one device
+// buffer (round.cu).  key identifies the member list and settings the tables
+// were built for; exec holds the round captured as a graph, once replayed.
+struct RoundPlan {
+  std::vector<uint64_t> key;
+  std::vector<unsigned char> host;
+  unsigned char *dev = nullptr;
+  size_t cap = 0;
+  struct Fp { int key, njobs, nabs, ncopy, nfp; size_t jobs, abs, copy, fpb; };
+  struct Fi { int n, fmt, store, njobs, nblk; size_t jobs, blk; };
+  struct Bp { int store, zf, variant, njobs, ntiles, max_views; size_t jobs, counter; };
+  std::vector<Fp> fp;
+  std::vector<Fi> fi;
+  std::vector<Bp> bp;
+  std::vector<tg_session *> fp_single, fi_single, bp_single;
+  cudaGraphExec_t exec = nullptr;
+  int launches = 0;  // kernels of one issue
+};
+int round_plan_build(RoundPlan &p, const std::vector<tg_session *> &ss, const std::vector<uint64_t> &key,
+                     cudaStream_t st);
+int round_plan_issue(RoundPlan &p, cudaStream_t st);
+int round_plan_launch_graph(RoundPlan &p, cudaStream_t st);
+void round_plan_release(RoundPlan &p, cudaStream_t st);
+void round_plan_signature(const std::vector<tg_session *> &ss, std::vector<uint64_t> &key);
+}  // namespace tg
+
 struct tg_batch {
   int dev = 0;
   cudaStream_t st = nullptr;
@@ -114,4 +143,7 @@ struct tg_batch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   tg_run_info info{};
   int rounds = 0, persistent_launches = 0;
+  uint64_t generation = 1;  // changes with the member list (plan keys)
+  tg::RoundPlan plan;       // the SIRT rounds' plan and graph
+  int graph_launches = 0;   // rounds of the last reconstruction replayed from a graph
 };

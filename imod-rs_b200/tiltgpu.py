@@ -185,6 +185,7 @@ EXTRA = {
                                          C.POINTER(_i32), C.POINTER(_i32)]),
     "tg_session_set_variant": (C.c_int, [_P, _i32]),
     "tg_variant_name": (C.c_char_p, [_i32]),
+    "tg_batch_plan_info": (C.c_int, [_P, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)]),
 }
 
 _lib = None
@@ -388,6 +389,13 @@ class Batch:
         ri = RunInfo()
         check(lib().tg_batch_last_run(self.h, C.byref(ri)))
         return {k: getattr(ri, k) for k, _ in RunInfo._fields_}
+
+    def plan_info(self):
+        """SIRT rounds of the last reconstruction: rounds replayed from a CUDA graph,
+        grouped reprojection / filter launches and kernels per round."""
+        v = [_i32() for _ in range(4)]
+        check(lib().tg_batch_plan_info(self.h, *[C.byref(x) for x in v]))
+        return dict(zip(("graph_rounds", "fp_groups", "filter_groups", "round_launches"), (x.value for x in v)))
 
     def close(self):
         if self.h:
