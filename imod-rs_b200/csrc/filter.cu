@@ -357,6 +357,15 @@ template <int R, bool INV> __device__ __forceinline__ void dft_r(float2 *v) {
   else bfly<R, INV>(v, nullptr, R);
 }
 
+// Shared-memory position of row element e: an XOR swizzle inside each group of
+// 16 complex values (128 bytes, one pass over the 32 banks).  The radix-8 passes
+// at spans 1 and 8 write with strides of 8 and 64 values, which unswizzled put
+// 16 and 4 lanes of a warp on the same banks; with the group index XORed into
+// the low bits every bank pair takes exactly two of a warp's 32 stores, and
+// reads of consecutive elements stay conflict-free.  A bijection on [0, N) for
+// N a multiple of 16 (every length these kernels take).
+__device__ __forceinline__ int swz(int e) { return e ^ ((e >> 4) & 15); }
+
 // Radix of the pass that starts at span NS, for V values per thread: 8, 4 or 2
 // while N/NS allows it (and V is a multiple), the factor 3 of 3*2^k lengths last.
 template <int N, int NS, int V> struct PassRadix {
@@ -390,7 +399,7 @@ __device__ __forceinline__ void p2_pass(const float2 (&x)[V], int t, const float
     dft_r<R, INV>(v);
     const int base = (b - k) * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) Y[base + r * NS] = v[r];
+    for (int r = 0; r < R; ++r) Y[swz(base + r * NS)] = v[r];
   }
 }
 
@@ -405,7 +414,7 @@ __device__ __forceinline__ float2 *p2_fft(float2 (&x)[V], int t, const float2 *_
   __syncthreads();
   if constexpr (NS * R < N) {
 #pragma unroll
-    for (int j = 0; j < V; ++j) x[j] = B[t + j * T];
+    for (int j = 0; j < V; ++j) x[j] = B[swz(t + j * T)];
     return p2_fft<N, V, NS * R, INV>(x, t, tw, B, A);
   } else {
     return B;
@@ -440,7 +449,7 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
   for (int j = 0; j < V; ++j) {  // x the radial weight while loading the inverse's first pass
     const int k = t + j * T;
     const float w = __ldg(&a.weights[k]);
-    const float2 z = F[k];
+    const float2 z = F[swz(k)];
     x[j] = make_float2(__fmul_rn(z.x, w), __fmul_rn(z.y, w));
   }
   // the inverse's first pass writes G (free since the forward's last barrier), not F,
@@ -451,7 +460,7 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
   const float inv_n = a.inv_n;
   const float stretch = a.stretch ? a.stretch[v] : 0.0f;
   auto sc = [&](int k) {
-    const float2 z = Rr[k];
+    const float2 z = Rr[swz(k)];
     return make_float2(__fmul_rn(z.x, inv_n), __fmul_rn(z.y, inv_n));
   };
   if (stretch != 0.0f) {
@@ -476,10 +485,10 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
       } else {
         o = make_float2(0.0f, 0.0f);
       }
-      S[k] = o;
+      S[swz(k)] = o;
     }
   } else {
-    for (int k = t; k < N; k += T) S[k] = sc(k);
+    for (int k = t; k < N; k += T) S[swz(k)] = sc(k);
   }
   __syncthreads();
   // pack into the staging format with the reference's fill rule (main.rs:386-406)
@@ -487,12 +496,12 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
   float hmax = 0.0f;  // largest |value| packed into FP16 by this thread
   auto pair = [&](int k, float2 &lo, float2 &hi) {  // (row[k], row[k+1]) of both rows, or the fill
     if (k >= 0 && k + 1 < N) {
-      lo = S[k];
-      hi = S[k + 1];
+      lo = S[swz(k)];
+      hi = S[swz(k + 1)];
     } else {
       float2 f;
       if (a.fill_mode == TG_FILL_ZERO) f = make_float2(0.0f, 0.0f);
-      else if (a.fill_mode == TG_FILL_EDGE) f = k < 0 ? S[0] : S[N - 1];
+      else if (a.fill_mode == TG_FILL_EDGE) f = k < 0 ? S[swz(0)] : S[swz(N - 1)];
       else f = make_float2(fillv, fillv);
       lo = hi = f;
     }

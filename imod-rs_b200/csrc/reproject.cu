@@ -676,16 +676,16 @@ template <int S, bool HALF, bool XT, bool IL>
 static int launch_batch_t(const FpArgs *jobs, int njobs, const int *blk_abs, int nabs, const int *blk_copy,
                           int ncopy, const int *blk_fp, int nfp, cudaStream_t st) {
   int k = 0;
-  if (HALF) {
+  if constexpr (HALF) {
     fp_zero_maxbits_kernel<<<(njobs + 127) / 128, 128, 0, st>>>(jobs, njobs);
     absmax_batch_kernel<<<nabs, 256, 0, st>>>(FpBatchDev{jobs, blk_abs, njobs});
     k += 2;
   }
-  if (HALF || IL) {
+  if constexpr (HALF || IL) {
     fp_copy_batch_kernel<S, HALF, XT><<<ncopy, 256, 0, st>>>(FpBatchDev{jobs, blk_copy, njobs});
     ++k;
   }
-  if (HALF) fp_half_batch_kernel<S, XT><<<nfp, 128, 0, st>>>(FpBatchDev{jobs, blk_fp, njobs});
+  if constexpr (HALF) fp_half_batch_kernel<S, XT><<<nfp, 128, 0, st>>>(FpBatchDev{jobs, blk_fp, njobs});
   else fp_fast_batch_kernel<S, XT, IL><<<nfp, 128, 0, st>>>(FpBatchDev{jobs, blk_fp, njobs});
   return k + 1;
 }

@@ -20,6 +20,8 @@
 // launches alone can be captured: a plan whose member list and settings come
 // round after round unchanged is captured once and replayed with
 // cudaGraphLaunch.
+#include <stdlib.h>
+
 #include <algorithm>
 #include <map>
 #include <vector>
@@ -72,9 +74,11 @@ int round_plan_build(RoundPlan &p, const std::vector<tg_session *> &ss, const st
   p.launches = 0;
   // reprojection groups
   std::map<int, std::vector<FpArgs>> fpg;
+  // TG_ROUND_FP_SINGLE=1: every series' reprojection as its own launches (profiling)
+  const bool fp_single_only = getenv("TG_ROUND_FP_SINGLE") != nullptr;
   for (tg_session *s : ss) {
     FpArgs a = fp_args(s);
-    const int k = fp_batch_key(a);
+    const int k = fp_single_only ? -1 : fp_batch_key(a);
     if (k < 0) p.fp_single.push_back(s);
     else fpg[k].push_back(a);
   }
