@@ -55,7 +55,16 @@ def c1_workload():
                 n_beads=40)
 
 
-WORKLOADS = {"c2": c2_workload, "c1": c1_workload}
+def c2strip_workload():
+    """The large WBP geometry (2048 wide, 121 jittered views, thickness 800) on 256 rows:
+    the same per-slice work as the full series, with 2.3 GB on the device, for counter
+    captures (their DRAM bytes scale to the full series by 2048 / 256 rows)."""
+    w = c2_workload()
+    w.update(name="large plain WBP strip: 121 views 2048x256 -> 2048x256x800, RADIAL 0.35/0.035", ny=256)
+    return w
+
+
+WORKLOADS = {"c2": c2_workload, "c1": c1_workload, "c2strip": c2strip_workload}
 
 
 class ClockSampler:
