@@ -87,11 +87,23 @@ __global__ void means_final_kernel(const double *partials, long npix, int nviews
   means[v] = (float)(t / (double)npix);
 }
 
+__global__ void view_sums_kernel(const double *partials, int nviews, double *sums) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nviews) return;
+  double t = 0.0;
+  for (int c = 0; c < MEAN_CH; ++c) t += partials[(size_t)v * MEAN_CH + c];
+  sums[v] = t;
+}
+
 void launch_log_means(const float *raw, float *logd, int npix, int nviews, double *partials,
                       float *means, cudaStream_t st) {
   if (logd) log_sum_kernel<true><<<dim3(MEAN_CH, nviews), 256, 0, st>>>(raw, logd, npix, partials);
   else log_sum_kernel<false><<<dim3(MEAN_CH, nviews), 256, 0, st>>>(raw, nullptr, npix, partials);
-  means_final_kernel<<<(nviews + 127) / 128, 128, 0, st>>>(partials, npix, nviews, means);
+  if (means) means_final_kernel<<<(nviews + 127) / 128, 128, 0, st>>>(partials, npix, nviews, means);
+}
+
+void launch_view_sums(const double *partials, int nviews, double *sums, cudaStream_t st) {
+  view_sums_kernel<<<(nviews + 127) / 128, 128, 0, st>>>(partials, nviews, sums);
 }
 
 // ---------------------------------------------------------------------------

@@ -4,9 +4,8 @@
 // A round takes every member series one SIRT iteration further (the loop body
 // of apps/tilt/src/main.rs:919-975): reprojection, residual R-weighting, and
 // the relaxed back-projection update.  The plan groups the members:
-//   * reprojection: series with the same form (FP16 copy or FP32, rows per
-//     thread, x-tilt, interleaved copy) share one launch per phase (max|vol|,
-//     copy, projection) over a block table;
+//   * reprojection: each series' own launches (or, on request, series with the
+//     same form share one launch per phase over a block table);
 //   * residual filter: series with the same register-resident FFT width,
 //     staging format and precision share one launch;
 //   * back-projection: one persistent launch per (precision, z-factor) group
@@ -74,11 +73,17 @@ int round_plan_build(RoundPlan &p, const std::vector<tg_session *> &ss, const st
   p.launches = 0;
   // reprojection groups
   std::map<int, std::vector<FpArgs>> fpg;
-  // TG_ROUND_FP_SINGLE=1: every series' reprojection as its own launches (profiling)
-  const bool fp_single_only = getenv("TG_ROUND_FP_SINGLE") != nullptr;
+  // Reprojection: every series' own kernels inside the round (its arguments are
+  // kernel parameters, used straight from the constant bank), by default.  The
+  // grouped form (TG_ROUND_FP_BATCH=1: one launch per phase over a block table,
+  // arguments read into registers from shared memory) launches less but measured
+  // slower on the 64-series mix (FP16 2.93e12 vs 3.17e12, FP32 1.76e12 vs 2.07e12
+  // updates/s): these kernels are issue-bound, and the argument registers cost
+  // occupancy.
+  const bool fp_grouped = getenv("TG_ROUND_FP_BATCH") != nullptr;
   for (tg_session *s : ss) {
     FpArgs a = fp_args(s);
-    const int k = fp_single_only ? -1 : fp_batch_key(a);
+    const int k = fp_grouped ? fp_batch_key(a) : -1;
     if (k < 0) p.fp_single.push_back(s);
     else fpg[k].push_back(a);
   }

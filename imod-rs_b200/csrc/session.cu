@@ -414,7 +414,8 @@ FpArgs fp_args(tg_session *s) {
 int stage_front(tg_session *s, int *launches) {
   // every run starts from the uploaded projections: log10 into d_logd (--log) and the
   // per-view means, as main.rs:608-623 does before each reconstruction
-  launch_log_means(s->d_raw, s->d_logd, s->nx * s->ny, s->nz, s->d_mpart, s->d_means, s->st);
+  launch_log_means(s->d_raw, s->d_logd, s->nx * s->ny, s->nz, s->d_mpart, s->means_pinned ? nullptr : s->d_means,
+                   s->st);
   *launches += 2;
   launch_filter(filter_args(s, false), s->st);
   *launches += 1;
@@ -986,6 +987,34 @@ int tg_session_kernel_info(tg_session *s, int32_t *fast, int32_t *variant, int32
   if (fmt) *fmt = s->fmt;
   if (padL) *padL = s->padL;
   if (PW) *PW = s->PW;
+  return TG_OK;
+}
+
+int tg_session_view_sums(tg_session *s, double *sums) {
+  if (!s || !sums) return TG_ERR_INVALID_ARG;
+  if (!s->uploaded) { set_error("no projections uploaded"); return TG_ERR_INVALID_ARG; }
+  TG_CUDA(cudaSetDevice(s->dev));
+  double *d = nullptr;
+  TG_CUDA(cudaMallocAsync((void **)&d, (size_t)s->nz * sizeof(double), s->st));
+  launch_log_means(s->d_raw, s->d_logd, s->nx * s->ny, s->nz, s->d_mpart, nullptr, s->st);
+  launch_view_sums(s->d_mpart, s->nz, d, s->st);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sums, d, (size_t)s->nz * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+  cudaFreeAsync(d, s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  return e == cudaSuccess ? TG_OK : cuda_fail(e, "tg_session_view_sums");
+}
+
+int tg_session_set_view_means(tg_session *s, const float *means) {
+  if (!s) return TG_ERR_INVALID_ARG;
+  TG_CUDA(cudaSetDevice(s->dev));
+  if (!means) {
+    s->means_pinned = false;
+    return TG_OK;
+  }
+  TG_CUDA(cudaMemcpyAsync(s->d_means, means, (size_t)s->nz * sizeof(float), cudaMemcpyHostToDevice, s->st));
+  TG_CUDA(cudaStreamSynchronize(s->st));
+  s->means_pinned = true;
   return TG_OK;
 }
 

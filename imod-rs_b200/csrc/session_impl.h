@@ -60,6 +60,9 @@ struct tg_session {  // one tilt series resident on a device
   tg_run_info info{};
   cudaEvent_t ev[6] = {};
   cudaGraphExec_t sirt_exec = nullptr;
+  // view means given by the caller (tg_session_set_view_means): a Y slab of a series
+  // sharded over GPUs fills with the whole series' means
+  bool means_pinned = false;
   // bounded-wait settings of the fast back-projector (tg_session_inject_wait_fault)
   unsigned long long wait_limit_ns = 2000000000ull;
   int fault_skip_stage = -1;

@@ -36,8 +36,11 @@ struct StatPartial {
 
 // ---- log transform + per-view means (main.rs:608-623) ----
 // logd == nullptr: means of raw; else logd = log10(max(raw, 0.001)) and its means
+// (means == nullptr: partial sums only)
 void launch_log_means(const float *raw, float *logd, int npix, int nviews, double *partials,
                       float *means, cudaStream_t st);
+// per-view f64 sums from the partials of launch_log_means
+void launch_view_sums(const double *partials, int nviews, double *sums, cudaStream_t st);
 
 // ---- filter stage: R-weighting (main.rs:333-381), cosine stretch
 // (main.rs:446-488) and staging-format packing ----

@@ -53,6 +53,37 @@ def gather_stats(local, y0: int, group=None):
     return merged
 
 
+def whole_series_means(view_sums, nx: int, ny_total: int):
+    """Mean fill values of whole views from the per-view f64 sums of all slabs
+    (apps/tilt/src/main.rs:616-623: the f64 mean rounded to f32)."""
+    return (np.asarray(view_sums, np.float64) / float(nx * ny_total)).astype(np.float32)
+
+
+def all_reduce_sums(x, group=None):
+    """Element-wise sum of a float64 vector over the ranks."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.from_numpy(np.ascontiguousarray(x, np.float64)).clone()
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.numpy()
+
+
+def reconstruct_slab(proj_slab, angles, nx: int, ny_total: int, sum_views=all_reduce_sums, **opts):
+    """One rank's Y slab of a series through the CUDA path: upload the slab's rows,
+    add the per-view sums over the ranks (sum_views), pin the whole series' mean fill
+    values, reconstruct.  Returns the slab's volume and its per-slice statistics."""
+    import tiltgpu as T
+
+    nz, ny, _ = proj_slab.shape
+    with T.Session(nx, ny, nz, angles, **opts) as s:
+        s.upload(proj_slab)
+        s.set_view_means(whole_series_means(sum_views(s.view_sums()), nx, ny_total))
+        s.reconstruct()
+        vol, _ = s.download()
+    return vol, slice_stats(vol)
+
+
 def reduce_max(x: float, group=None) -> float:
     import torch
     import torch.distributed as dist

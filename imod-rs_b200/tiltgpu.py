@@ -159,6 +159,8 @@ EXPORTS = {
     "tg_ctf_correct_strip": (C.c_int, [_P, _P, C.POINTER(CtfStripParams), _i32]),
     "tg_upload_sections": (C.c_int, [_P, _i32, _i32, _P]),
     "tg_session_inject_wait_fault": (C.c_int, [_P, _i32, C.c_uint32]),
+    "tg_session_view_sums": (C.c_int, [_P, _P]),
+    "tg_session_set_view_means": (C.c_int, [_P, _P]),
     "tg_download_slices_f16_async": (C.c_int, [_P, _i32, _i32, _P]),
     "tg_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_P)]),
     "tg_host_free": (C.c_int, [_P]),
@@ -326,6 +328,17 @@ class Session:
             name = lib().tg_variant_name(variant).decode() + ("+xtilt-blend" if fast == 3 else "")
         return {"fast": fast == 1, "xtilt_split": fast == 3, "variant": variant,
                 "variant_name": name, "fmt": fmt, "padL": padl, "PW": pw}
+
+    def view_sums(self):
+        """Per-view f64 sums of the uploaded rows (after --log), for slab sharding."""
+        out = np.empty(self.nz, np.float64)
+        check(lib().tg_session_view_sums(self.h, _ptr(out)))
+        return out
+
+    def set_view_means(self, means):
+        """Pins the mean fill values (whole-series means of a slab); None: compute them again."""
+        m = None if means is None else _f32(means)
+        check(lib().tg_session_set_view_means(self.h, _ptr(m)))
 
     def inject_wait_fault(self, skip_stage=-1, wait_limit_us=0):
         """Test hook: the back-projector's producer leaves out one pipeline stage and

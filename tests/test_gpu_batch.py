@@ -70,10 +70,13 @@ SIRT_JOBS = [  # every reprojection form and filter width group, uneven iteratio
 ]
 
 
-def test_batched_sirt_rounds_grouped_and_graphed():
+@pytest.mark.parametrize("grouped_fp", [False, True])
+def test_batched_sirt_rounds_grouped_and_graphed(grouped_fp, monkeypatch):
     # SIRT rounds run as grouped reprojection / filter / back-projection launches,
     # replayed from a CUDA graph while the members stay the same; every series must
     # still come out bit-identical to its stand-alone reconstruction
+    if grouped_fp:  # reprojection of same-form series in one launch per phase
+        monkeypatch.setenv("TG_ROUND_FP_BATCH", "1")
     alone = []
     for i, job in enumerate(SIRT_JOBS):
         s = _make_relaxed(job, 100 + i)
@@ -92,7 +95,7 @@ def test_batched_sirt_rounds_grouped_and_graphed():
             assert sb["amin"] == sa["amin"] and sb["amax"] == sa["amax"]
     info = b.plan_info()
     assert info["graph_rounds"] == 3          # rounds 1..3, one plan per member list
-    assert info["fp_groups"] >= 2 and info["filter_groups"] >= 1
+    assert (info["fp_groups"] >= 2) == grouped_fp and info["filter_groups"] >= 1
     b.close()
     for s in sessions:
         s.close()
