@@ -160,16 +160,22 @@ def hbm_peak():
     return 6650.0, "of fallback (6.65 TB/s, MEASURED_PEAKS.json absent)"
 
 
-def read_traffic():
-    """Per-launch DRAM traffic of the back-projection kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "bp_fast_c2_fp16.md")
+def read_traffic(variant_name, storage="fp16"):
+    """Per-launch DRAM bytes of the back-projection kernel at the large configuration,
+    from the committed ncu summary of that tile variant (a 256-row strip of the same
+    geometry, scaled by 2048 / 256 rows), or None when the timed variant has none."""
+    path = os.path.join(ROOT, "profiles", f"bp_fast_c2strip_{storage}.md")
+    vals = {}
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].strip())
+            if ":" in line and line.split(":", 1)[0] in ("variant", "traffic_bytes_per_launch"):
+                k, v = line.split(":", 1)
+                vals[k] = v.strip()
     except OSError:
-        pass
-    return None
+        return None
+    if vals.get("variant") != variant_name or "traffic_bytes_per_launch" not in vals:
+        return None
+    return float(vals["traffic_bytes_per_launch"])
 
 
 def run_ours(args):
@@ -310,7 +316,7 @@ def run_ours(args):
     bp_s = r16["bp_ms"] * 1e-3
     ach = upd_pass * 4.0 / bp_s / 1e9
     peak = SM_COUNT * SMEM_BYTES_PER_CLK * sm_mhz * 1e6 / 1e9
-    traffic = read_traffic()
+    traffic = read_traffic(r16["kernel"]["variant_name"])
     line = {
         "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r16["ms"] / args.steps, "higher_is_better": True,
@@ -329,7 +335,9 @@ def run_ours(args):
         "roofline": {"bound": "smem", "achieved": ach, "peak": peak, "unit": "GB/s",
                      "frac": ach / peak, "traffic": traffic,
                      "note": "shared-memory bytes of the back-projection kernel (4 B/update FP16 pair); "
-                             "peak = 148 SMs x 128 B/clk x median SM clock sampled in the run"},
+                             "peak = 148 SMs x 128 B/clk x median SM clock sampled in the run; traffic = "
+                             "DRAM bytes per launch of this tile variant from profiles/bp_fast_c2strip_fp16.md "
+                             "(ncu on a 256-row strip of the same geometry, x 2048/256), null if untuned"},
         "roofline_hbm": {"bound": "hbm", "achieved": (4.0 * nz * nx * ny + 4.0 * onx * onz * ny) / bp_s / 1e9,
                          "peak": hbm_peak()[0], "unit": "GB/s",
                          "note": "back-projection kernel: FP16 staged rows (4 B per sample: value and "

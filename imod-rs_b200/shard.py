@@ -72,7 +72,9 @@ def all_reduce_sums(x, group=None):
 def reconstruct_slab(proj_slab, angles, nx: int, ny_total: int, sum_views=all_reduce_sums, **opts):
     """One rank's Y slab of a series through the CUDA path: upload the slab's rows,
     add the per-view sums over the ranks (sum_views), pin the whole series' mean fill
-    values, reconstruct.  Returns the slab's volume and its per-slice statistics."""
+    values, reconstruct.  Returns the slab's volume and its per-slice statistics.
+    Not for x-tilt, local alignment or fake SIRT (their rows or slices reach across
+    slab edges)."""
     import tiltgpu as T
 
     nz, ny, _ = proj_slab.shape
