@@ -853,6 +853,53 @@ def c4_at_once(budget_gb=150.0, pool=None):
             "wall_s": sv["wall_s"], "serial_s": sum(service), "unit": "updates/s"}
 
 
+def run_cli(args):
+    """The drop-in `tilt` command on the large WBP series, files in and out: a 2.0 GB
+    float MRC stack and its .tlt written to a scratch directory, then `bin/tilt` run
+    (overlapped read/upload and download/write) with mode-2 and mode-12 output; wall
+    clock of the whole command against the device-resident rate."""
+    import shutil
+    import tempfile
+
+    import torch
+
+    import tiltgpu as T
+    torch.cuda.set_device(0)
+    w = c2_workload()
+    nx, ny, onz, ang = w["nx"], w["ny"], w["onz"], w["angles"]
+    nz = len(ang)
+    d = torch.empty(nz * ny * nx, dtype=torch.float32, device="cuda")
+    T.synth_projections(ang, nx=nx, ny=ny, vol_nx=nx, vol_nz=onz, n_ell=w["n_ell"], rmin=3, rmax=40, dmin=0.2,
+                        dmax=1.0, n_beads=w["n_beads"], bead_r=5, bead_d=5.0, noise_kind=2, noise=20000.0,
+                        seed=1000, out_device_ptr=d.data_ptr())
+    proj = d.cpu().numpy().reshape(nz, ny, nx)
+    del d
+    torch.cuda.empty_cache()
+    tmp = tempfile.mkdtemp(prefix="tilt_cli_", dir=args.scratch or None)
+    res = {"workload": w["name"] + ", through bin/tilt (MRC in, MRC out, --log)", "unit": "updates/s"}
+    try:
+        src, tlt = os.path.join(tmp, "in.mrc"), os.path.join(tmp, "in.tlt")
+        T.mrc_write_f32(src, T.mrc_header_new(nx, ny, nz, "Float"), proj)
+        T.write_tilt_file(tlt, ang)
+        upd = float(nx) * onz * ny * nz
+        for mode in (2, 12):
+            out = os.path.join(tmp, f"out{mode}.rec")
+            t0 = time.perf_counter()
+            r = subprocess.run([T.CLI_PATH, "-i", src, "-o", out, "-t", tlt, "-z", str(onz), "--radial",
+                                "0.35,0.035", "--log", "--storage", "fp16", "--mode", str(mode)],
+                               capture_output=True, text=True)
+            wall = time.perf_counter() - t0
+            stages = [ln for ln in r.stderr.splitlines() if ln.startswith("tilt: read+upload")]
+            res[f"mode{mode}"] = {"rc": r.returncode, "wall_s": wall, "value": upd / wall,
+                                  "output_bytes": os.path.getsize(out) if os.path.exists(out) else None,
+                                  "stages": stages[-1] if stages else r.stderr[-300:]}
+            if os.path.exists(out):
+                os.remove(out)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    print(json.dumps(res), flush=True)
+
+
 def run_serve(args):
     import torch
     torch.cuda.set_device(0)
@@ -867,7 +914,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c3", "c4", "serve"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c3", "c4", "serve", "cli"])
     ap.add_argument("--sirt", type=int, default=20, help="c3: SIRT iterations")
     ap.add_argument("--xtilt", type=float, default=1.5, help="c3: x-axis tilt of every view (deg)")
     ap.add_argument("--sirt-relax", type=float, default=1.0, help="c3: SIRT relaxation (the reference's default 1.0)")
@@ -881,6 +928,7 @@ def main():
     ap.add_argument("--saturated-seconds", type=float, default=15.0,
                     help="default run: seconds of the saturated (40 jobs/s) served stream")
     ap.add_argument("--no-serving", action="store_true", help="default run: skip the served streams and C4")
+    ap.add_argument("--scratch", default=None, help="cli: directory for the MRC files (default: the system temp)")
     ap.add_argument("--forms", default=None, help="staging precisions to time (c1/c2: fp32,fp16; c3: fp32,bf16)")
     ap.add_argument("--profile", action="store_true",
                     help="time the requested forms only (no e2e, no CPU baseline); for ncu captures")
@@ -899,6 +947,9 @@ def main():
         return
     if args.workload == "serve":
         run_serve(args)
+        return
+    if args.workload == "cli":
+        run_cli(args)
         return
     if args.impl == "reference":
         run_reference(args)
