@@ -369,14 +369,21 @@ template <int R, bool INV> __device__ __forceinline__ void dft_r(float2 *v) {
   else bfly<R, INV>(v, nullptr, R);
 }
 
-// Shared-memory position of row element e: an XOR swizzle inside each group of
-// 16 complex values (128 bytes, one pass over the 32 banks).  The radix-8 passes
-// at spans 1 and 8 write with strides of 8 and 64 values, which unswizzled put
-// 16 and 4 lanes of a warp on the same banks; with the group index XORed into
-// the low bits every bank pair takes exactly two of a warp's 32 stores, and
-// reads of consecutive elements stay conflict-free.  A bijection on [0, N) for
-// N a multiple of 16 (every length these kernels take).
-__device__ __forceinline__ int swz(int e) { return e ^ ((e >> 4) & 15); }
+// Shared-memory position of row element e: one padding slot after every 16
+// complex values (128 bytes, one pass over the 32 banks).  Unpadded, the radix-8
+// passes at spans 1 and 8 store with strides of 8 and 64 values, which put 16 and
+// 4 lanes of a warp on the same banks; padded, every bank pair takes exactly two
+// of a warp's 32 stores in every pass, and reads of consecutive elements stay
+// conflict-free.  A pass's R outputs sit at e + r*NS with the low four bits of e
+// and r*NS never carrying into bit 4, so their padded positions are one base plus
+// compile-time offsets (no per-element address arithmetic).
+__device__ __forceinline__ int swz(int e) { return e + (e >> 4); }
+// swz(e + off) for an offset whose low four bits never carry with e's: both the
+// pass outputs e = base + r*NS (base's low bits stay below 16 - (r*NS mod 16):
+// base - k is a multiple of NS*R and k < NS) and the reads t + j*T (T a multiple
+// of 16) -- so the offset is a compile-time constant.
+__device__ __forceinline__ int swz_add(int swz_e, int off) { return swz_e + off + (off >> 4); }
+template <int N> __host__ __device__ constexpr int padded_len() { return N + N / 16; }
 
 // Radix of the pass that starts at span NS, for V values per thread: 8, 4 or 2
 // while N/NS allows it (and V is a multiple), the factor 3 of 3*2^k lengths last.
@@ -409,9 +416,9 @@ __device__ __forceinline__ void p2_pass(const float2 (&x)[V], int t, const float
       }
     }
     dft_r<R, INV>(v);
-    const int base = (b - k) * R + k;
+    const int sb = swz((b - k) * R + k);
 #pragma unroll
-    for (int r = 0; r < R; ++r) Y[swz(base + r * NS)] = v[r];
+    for (int r = 0; r < R; ++r) Y[swz_add(sb, r * NS)] = v[r];
   }
 }
 
@@ -426,7 +433,7 @@ __device__ __forceinline__ float2 *p2_fft(float2 (&x)[V], int t, const float2 *_
   __syncthreads();
   if constexpr (NS * R < N) {
 #pragma unroll
-    for (int j = 0; j < V; ++j) x[j] = B[swz(t + j * T)];
+    for (int j = 0; j < V; ++j) x[j] = B[swz_add(swz(t), j * T)];
     return p2_fft<N, V, NS * R, INV>(x, t, tw, B, A);
   } else {
     return B;
@@ -438,7 +445,7 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
   extern __shared__ __align__(16) unsigned char fsm[];
   constexpr int T = N / V;
   float2 *A = reinterpret_cast<float2 *>(fsm);
-  float2 *B = A + N;
+  float2 *B = A + padded_len<N>();
   const int t = threadIdx.x;
   const int r0 = 2 * jp;
   const bool has1 = r0 + 1 < a.ny;
@@ -461,7 +468,7 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
   for (int j = 0; j < V; ++j) {  // x the radial weight while loading the inverse's first pass
     const int k = t + j * T;
     const float w = __ldg(&a.weights[k]);
-    const float2 z = F[swz(k)];
+    const float2 z = F[swz_add(swz(t), j * T)];
     x[j] = make_float2(__fmul_rn(z.x, w), __fmul_rn(z.y, w));
   }
   // the inverse's first pass writes G (free since the forward's last barrier), not F,
@@ -592,7 +599,7 @@ __global__ void __launch_bounds__(N / V) filter_p2_batch_kernel(FilterBatchDev f
 }
 
 template <int N, int V, int FMT, int STORE> static void launch_p2(const FilterArgs &a, cudaStream_t st) {
-  const size_t smem = (size_t)N * 16;
+  const size_t smem = (size_t)padded_len<N>() * 16;
   auto k = filter_p2_kernel<N, V, FMT, STORE>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k<<<dim3((a.ny + 1) / 2, a.nviews), N / V, smem, st>>>(a);
@@ -632,7 +639,7 @@ int filter_batch_width(const FilterArgs &a) {
 
 template <int N, int V, int FMT, int STORE>
 static void launch_p2_batch(const FilterBatchDev &fb, int nblocks, cudaStream_t st) {
-  const size_t smem = (size_t)N * 16;
+  const size_t smem = (size_t)padded_len<N>() * 16;
   auto k = filter_p2_batch_kernel<N, V, FMT, STORE>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k<<<nblocks, N / V, smem, st>>>(fb);
