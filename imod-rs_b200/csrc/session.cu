@@ -328,8 +328,8 @@ int launch_bp(tg_session *s, int mode, int *ntiles) {
   return launch_bp_general(a, s->store, s->st, ntiles);
 }
 
-// Times each fast tile variant once on this series and keeps the fastest
-// (process-wide cache keyed by the series shape).
+// Times each fast tile variant once on (the first 64 slices of) this series and
+// keeps the fastest (process-wide cache keyed by the series shape).
 int autotune(tg_session *s) {
   if (!s->fast && !s->xt_split) { s->variant = 0; return TG_OK; }
   if (const char *env = getenv("TG_BP_VARIANT")) {  // fixed tile shape (profiling, tuning)
@@ -351,6 +351,10 @@ int autotune(tg_session *s) {
     BpArgs a = bp_args(s, 1);
     a.wait_limit_ns = 2000000000ull;  // tuning never runs the test hook
     a.fault_skip_stage = -1;
+    // the first 64 slices (every tile shape's rows divide 64): the time per update does
+    // not depend on the slice, and a one-shot reconstruction should not pay for tuning
+    // that is longer than the reconstruction itself
+    a.ny = std::min(a.ny, 64);
     if (s->xt_split) a.vol = s->xtb;
     int nt = 0;
     // warm + timed launch (mode 1 writes the volume, which is rewritten afterwards)
