@@ -614,10 +614,6 @@ static const FastVariant kFast[] = {
 };
 constexpr int MAX_S = 16;  // rows per tile of the widest variant (sizes the staging buffer)
 int bp_fast_variants() { return (int)(sizeof(kFast) / sizeof(kFast[0])); }
-// 1 for the variants whose FP16 form sums a stage's 4 views in half precision: their
-// FP16 results differ in rounding from the other variants' (which all add view by
-// view), so a batched launch only groups series whose variants agree on it
-int bp_fast_variant_hs(int v) { return v == 14 || v == 15 ? 1 : 0; }
 const char *bp_fast_variant_name(int v) { return kFast[v].name; }
 int bp_fast_row_align() { return MAX_S; }
 

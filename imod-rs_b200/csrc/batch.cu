@@ -9,7 +9,6 @@
 // batch, so each series' volume is bit-identical to its stand-alone result.
 #include <algorithm>
 #include <map>
-#include <tuple>
 #include <vector>
 
 #include "session_impl.h"
@@ -24,13 +23,9 @@ namespace tg {
 int batch_bp(tg_batch *b, const std::vector<tg_session *> &ss, const std::vector<int> &modes,
              std::vector<int> &ntiles, int *launches) {
   ntiles.assign(ss.size(), 0);
-  // groups: (staging precision, z-factor, half partial sums); series of one group share a launch
-  std::map<std::tuple<int, int, int>, std::vector<int>> groups;
+  std::map<std::pair<int, int>, std::vector<int>> groups;
   for (size_t i = 0; i < ss.size(); ++i) {
-    if (ss[i]->fast)
-      groups[std::make_tuple(ss[i]->store, ss[i]->zf_any ? 1 : 0,
-                             ss[i]->store == TG_STORE_FP16 ? bp_fast_variant_hs(std::max(0, ss[i]->variant)) : 0)]
-          .push_back((int)i);
+    if (ss[i]->fast) groups[{ss[i]->store, ss[i]->zf_any ? 1 : 0}].push_back((int)i);
     else {
       int rc = launch_bp(ss[i], modes[i], &ntiles[i]);
       if (rc != TG_OK) return rc;
@@ -73,7 +68,7 @@ int batch_bp(tg_batch *b, const std::vector<tg_session *> &ss, const std::vector
     bl.ntiles = (int)total;
     bl.counter = b->d_counter;
     bl.max_views = max_views;
-    int rc = launch_bp_batch(bl, std::get<0>(kv.first), std::get<1>(kv.first) != 0, variant, b->st);
+    int rc = launch_bp_batch(bl, kv.first.first, kv.first.second != 0, variant, b->st);
     if (rc != TG_OK) return rc;
     TG_CUDA(cudaGetLastError());
     ++*launches;

@@ -127,7 +127,6 @@ struct BatchLaunch {
 };
 int launch_bp_batch(const BatchLaunch &bl, int store, bool zf, int variant, cudaStream_t st);
 void bp_fast_tile_shape(int variant, int *S, int *TX, int *TZ);
-int bp_fast_variant_hs(int variant);
 struct BpTile { int S, K, TX, NT, VPS, wmax; };
 // Fast kernel: no x-tilt, no local alignment, ROWPAIR format.
 // zf: 0 none, 1 z-factors, 2 z-factors and one x-tilt in the positions (row sums)
