@@ -219,13 +219,7 @@ template <class C> struct SmemLayout {
 // stage whose copies were issued; skipped = a stage left out by the test hook (-1).
 struct ProducerState { int issued = 0, skipped = -1; };
 
-// HS (FP16 staging only): the HFMA2 results of one stage's views are summed in
-// half precision per (row pair, depth) and added to the FP32 accumulators once per
-// stage instead of once per view (two mixed-precision adds per row pair and stage).
-// The half partial holds at most VPS <= 4 interpolated values, each below the FP16
-// staging limit for summed values (FP16_SUM_LIMIT, checked by the filter), so it
-// cannot overflow.
-template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF, int HS = 0>
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
 __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz, unsigned char *sm,
                                         const SmemLayout<FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>> &L,
                                         int &gst, volatile int *s_abort_p, ProducerState &ps) {
@@ -339,10 +333,6 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
 #pragma unroll
   for (int j = 0; j < K; ++j) dz[j] = __fsub_rn((float)min(oz0 + tzg + j * OZG, a.onz - 1), a.cz);
 
-  constexpr bool HSUM = HS && STORE == TG_STORE_FP16;
-  static_assert(!HSUM || VPS <= 4, "half partial sums of at most 4 views");
-  __half2 ph[HSUM ? SP : 1][HSUM ? K : 1];
-
   bool ok = true;
   for (int st = 0; st < nst && ok; ++st) {
     const int g = g0 + st, b = g % NSTAGE;
@@ -397,12 +387,7 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
               const uint2 e = lds64i<sp * WMAX * 8>(addr);
               const __half2 r = __hfma2(f2, *reinterpret_cast<const __half2 *>(&e.y),
                                         *reinterpret_cast<const __half2 *>(&e.x));
-              if constexpr (HSUM) {
-                if (vi == 0) ph[sp][j] = r;  // every stage has at least one view
-                else ph[sp][j] = __hadd2(ph[sp][j], r);
-              } else {
-                add2_f32_f16(acc[2 * sp][j], acc[2 * sp + 1][j], *reinterpret_cast<const uint32_t *>(&r));
-              }
+              add2_f32_f16(acc[2 * sp][j], acc[2 * sp + 1][j], *reinterpret_cast<const uint32_t *>(&r));
             });
           } else {
             const __nv_bfloat162 f2 = __float2bfloat162_rn(f0);
@@ -419,13 +404,6 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
     }
     __syncwarp();
     if ((tid & 31) == 0) mbar_arrive(smem_u32(&empty[b]));  // this warp is done with buffer b
-    if constexpr (HSUM) {
-#pragma unroll
-      for (int j = 0; j < K; ++j)
-#pragma unroll
-        for (int sp = 0; sp < SP; ++sp)
-          add2_f32_f16(acc[2 * sp][j], acc[2 * sp + 1][j], *reinterpret_cast<const uint32_t *>(&ph[sp][j]));
-    }
   }
   __syncwarp();       // lanes that left the loop at different stages reconverge
   consumer_sync(NT);  // all consumers past the loop (buffers free, abort flag settled)
@@ -529,8 +507,8 @@ template <class C> __device__ __forceinline__ void drain_ring(const SmemLayout<C
 }
 
 // One launch per series: grid = tiles of that series.
-template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF, int HS = 0>
-__global__ void __launch_bounds__(NT + 32, HS ? 3 : 1) bp_fast_kernel(const __grid_constant__ BpArgs a) {
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
+__global__ void __launch_bounds__(NT + 32) bp_fast_kernel(const __grid_constant__ BpArgs a) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   extern __shared__ __align__(128) unsigned char sm[];
   __shared__ volatile int s_abort;
@@ -538,7 +516,7 @@ __global__ void __launch_bounds__(NT + 32, HS ? 3 : 1) bp_fast_kernel(const __gr
   init_ring(L, &s_abort);
   int gst = 0;
   ProducerState ps;
-  bp_tile<STORE, S, K, TX, NT, VPS, NSTAGE, ZF, HS>(a, blockIdx.x, blockIdx.y, blockIdx.z, sm, L, gst, &s_abort, ps);
+  bp_tile<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>(a, blockIdx.x, blockIdx.y, blockIdx.z, sm, L, gst, &s_abort, ps);
   drain_ring(L, ps, &s_abort, a.wait_limit_ns);
 }
 
@@ -546,8 +524,8 @@ __global__ void __launch_bounds__(NT + 32, HS ? 3 : 1) bp_fast_kernel(const __gr
 // tile of the queue (longest series first) until it is empty.  Each tile's
 // arithmetic is the same as in the per-series kernel, so every series' result
 // does not depend on what else is in the batch.
-template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF, int HS = 0>
-__global__ void __launch_bounds__(NT + 32, HS ? 3 : 1) bp_batch_kernel(const BpArgs *__restrict__ jobs, int njobs,
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
+__global__ void __launch_bounds__(NT + 32) bp_batch_kernel(const BpArgs *__restrict__ jobs, int njobs,
                                                            int ntiles, int *counter, int max_views) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   extern __shared__ __align__(128) unsigned char sm[];
@@ -582,7 +560,7 @@ __global__ void __launch_bounds__(NT + 32, HS ? 3 : 1) bp_batch_kernel(const BpA
     const int nbx = s_args.nbx, nxz = s_args.ntiles_xz;
     const int bx = T.z % nbx, by = (T.z % nxz) / nbx, bz = T.z / nxz;
     limit_ns = s_args.wait_limit_ns;
-    if (!bp_tile<STORE, S, K, TX, NT, VPS, NSTAGE, ZF, HS>(s_args, bx, by, bz, sm, L, gst, &s_abort, ps)) {
+    if (!bp_tile<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>(s_args, bx, by, bz, sm, L, gst, &s_abort, ps)) {
       s_abort = 1;
     }
   }
@@ -608,19 +586,16 @@ static const FastVariant kFast[] = {
     {8, 4, 64, 256, 4, 3, "S8K4TX64NT256V4N3"},
     {16, 2, 64, 256, 4, 3, "S16K2TX64NT256V4N3"},
     {16, 2, 32, 256, 4, 3, "S16K2TX32NT256V4N3"},
-    // half partial sums per stage (FP16 staging; the same as variant 11 for FP32/BF16)
-    {8, 4, 64, 256, 4, 3, "S8K4TX64NT256V4N3H"},
-    {8, 4, 32, 256, 4, 3, "S8K4TX32NT256V4N3H"},
 };
 constexpr int MAX_S = 16;  // rows per tile of the widest variant (sizes the staging buffer)
 int bp_fast_variants() { return (int)(sizeof(kFast) / sizeof(kFast[0])); }
 const char *bp_fast_variant_name(int v) { return kFast[v].name; }
 int bp_fast_row_align() { return MAX_S; }
 
-template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF, int HS = 0>
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
 static int launch_fast_t(const BpArgs &a0, cudaStream_t st, int *ntiles) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
-  auto kern = bp_fast_kernel<STORE, S, K, TX, NT, VPS, NSTAGE, ZF, HS>;
+  auto kern = bp_fast_kernel<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   size_t smem = C::smem(a0.nviews);
   if (smem > 220 * 1024) return TG_ERR_UNSUPPORTED;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -634,10 +609,10 @@ static int launch_fast_t(const BpArgs &a0, cudaStream_t st, int *ntiles) {
   return TG_OK;
 }
 
-template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF, int HS = 0>
+template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
 static int launch_batch_t(const BatchLaunch &bl, cudaStream_t st) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
-  auto kern = bp_batch_kernel<STORE, S, K, TX, NT, VPS, NSTAGE, ZF, HS>;
+  auto kern = bp_batch_kernel<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   size_t smem = C::smem(bl.max_views);
   if (smem > 220 * 1024) return TG_ERR_UNSUPPORTED;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -670,8 +645,6 @@ static int launch_fast_v(const BpArgs &a, int variant, cudaStream_t st, int *nti
     case 10: return launch_fast_t<STORE, 8, 4, 32, 256, 8, 3, ZF>(a, st, ntiles);
     case 12: return launch_fast_t<STORE, 16, 2, 64, 256, 4, 3, ZF>(a, st, ntiles);
     case 13: return launch_fast_t<STORE, 16, 2, 32, 256, 4, 3, ZF>(a, st, ntiles);
-    case 14: return launch_fast_t<STORE, 8, 4, 64, 256, 4, 3, ZF, STORE == TG_STORE_FP16>(a, st, ntiles);
-    case 15: return launch_fast_t<STORE, 8, 4, 32, 256, 4, 3, ZF, STORE == TG_STORE_FP16>(a, st, ntiles);
     default: return launch_fast_t<STORE, 8, 4, 64, 256, 4, 3, ZF>(a, st, ntiles);
   }
 }
@@ -692,8 +665,6 @@ static int launch_batch_v(const BatchLaunch &bl, int variant, cudaStream_t st) {
     case 10: return launch_batch_t<STORE, 8, 4, 32, 256, 8, 3, ZF>(bl, st);
     case 12: return launch_batch_t<STORE, 16, 2, 64, 256, 4, 3, ZF>(bl, st);
     case 13: return launch_batch_t<STORE, 16, 2, 32, 256, 4, 3, ZF>(bl, st);
-    case 14: return launch_batch_t<STORE, 8, 4, 64, 256, 4, 3, ZF, STORE == TG_STORE_FP16>(bl, st);
-    case 15: return launch_batch_t<STORE, 8, 4, 32, 256, 4, 3, ZF, STORE == TG_STORE_FP16>(bl, st);
     default: return launch_batch_t<STORE, 8, 4, 64, 256, 4, 3, ZF>(bl, st);
   }
 }

@@ -162,24 +162,16 @@ template <> struct Pack<TG_STORE_BF16> {
   }
 };
 
-// FP16 staging holds the filtered values below FP16_SUM_LIMIT: the back-projector
-// may sum up to four interpolated values of consecutive views in half precision
-// (4 x 16000 plus rounding stays below the largest half, 65504); the differences
-// b - a only need to be finite halves (|d| < 65520).  Every packed value's
-// magnitude is tracked (values in .x, differences in .y); a row that does not fit
-// sets bit 2 of the session's error word, which the host reports as TG_ERR_RANGE
-// (a diverging SIRT run whose residuals outgrow FP16; FP32 and BF16 staging have
-// the f32 range).
-constexpr float FP16_SUM_LIMIT = 16000.0f, FP16_LIMIT = 65520.0f;
-template <int STORE> __device__ __forceinline__ void range_track(float2 &mx, float v0, float v1, bool diff) {
-  if (STORE == TG_STORE_FP16) {
-    const float m = fmaxf(fabsf(v0), fabsf(v1));
-    if (diff) mx.y = fmaxf(mx.y, m);
-    else mx.x = fmaxf(mx.x, m);
-  }
+// FP16 staging holds |v| < 65520 (larger values round to infinity).  Every packed
+// value's magnitude is tracked; a row that does not fit sets bit 2 of the
+// session's error word, which the host reports as TG_ERR_RANGE (a diverging SIRT
+// run whose residuals outgrow FP16; FP32 and BF16 staging have the f32 range).
+constexpr float FP16_LIMIT = 65520.0f;
+template <int STORE> __device__ __forceinline__ void range_track(float &mx, float v0, float v1) {
+  if (STORE == TG_STORE_FP16) mx = fmaxf(mx, fmaxf(fabsf(v0), fabsf(v1)));
 }
-template <int STORE> __device__ __forceinline__ void range_report(const FilterArgs &a, float2 mx) {
-  if (STORE == TG_STORE_FP16 && (mx.x >= FP16_SUM_LIMIT || mx.y >= FP16_LIMIT) && a.err) atomicOr(a.err, 4);
+template <int STORE> __device__ __forceinline__ void range_report(const FilterArgs &a, float mx) {
+  if (STORE == TG_STORE_FP16 && mx >= FP16_LIMIT && a.err) atomicOr(a.err, 4);
 }
 
 // Value pair (a, b) of element k of a final row, with the reference's fill
@@ -279,7 +271,7 @@ __global__ void __launch_bounds__(256) filter_kernel(FilterArgs a) {
     row1 = s1;
   }
   const float fillv = a.fill ? a.fill[v] : 0.0f;
-  float2 hmax = make_float2(0.0f, 0.0f);  // largest |value| and |difference| packed into FP16
+  float hmax = 0.0f;  // largest |value| packed into FP16 by this thread
   if (FMT == FMT_ROWS) {  // plain filtered rows written back over the input rows
     float *o0 = reinterpret_cast<float *>(a.out) + ((size_t)v * a.ny + r0) * n;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -302,8 +294,8 @@ __global__ void __launch_bounds__(256) filter_kernel(FilterArgs a) {
       } else {
         uint2 w;
         const float d0 = __fsub_rn(b0, a0), d1 = __fsub_rn(b1, a1);
-        range_track<STORE>(hmax, a0, a1, false);
-        range_track<STORE>(hmax, d0, d1, true);
+        range_track<STORE>(hmax, a0, a1);
+        range_track<STORE>(hmax, d0, d1);
         w.x = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(a0, a1);
         w.y = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(d0, d1);
         reinterpret_cast<uint2 *>(out)[e] = w;
@@ -324,12 +316,8 @@ __global__ void __launch_bounds__(256) filter_kernel(FilterArgs a) {
         if (has1) reinterpret_cast<float2 *>(o1)[e] = make_float2(a1, b1);
       } else {
         const float d0 = __fsub_rn(b0, a0), d1 = __fsub_rn(b1, a1);
-        range_track<STORE>(hmax, a0, a0, false);
-        range_track<STORE>(hmax, d0, d0, true);
-        if (has1) {
-          range_track<STORE>(hmax, a1, a1, false);
-          range_track<STORE>(hmax, d1, d1, true);
-        }
+        range_track<STORE>(hmax, a0, d0);
+        if (has1) range_track<STORE>(hmax, a1, d1);
         reinterpret_cast<uint32_t *>(o0)[e] = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(a0, d0);
         if (has1)
           reinterpret_cast<uint32_t *>(o1)[e] = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(a1, d1);
@@ -524,7 +512,7 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
   __syncthreads();
   // pack into the staging format with the reference's fill rule (main.rs:386-406)
   const float fillv = a.fill ? a.fill[v] : 0.0f;
-  float2 hmax = make_float2(0.0f, 0.0f);  // largest |value| and |difference| packed into FP16
+  float hmax = 0.0f;  // largest |value| packed into FP16 by this thread
   auto pair = [&](int k, float2 &lo, float2 &hi) {  // (row[k], row[k+1]) of both rows, or the fill
     if (k >= 0 && k + 1 < N) {
       lo = S[swz(k)];
@@ -549,8 +537,8 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
       } else {
         uint2 w;
         const float d0 = __fsub_rn(hi.x, lo.x), d1 = __fsub_rn(hi.y, lo.y);
-        range_track<STORE>(hmax, lo.x, lo.y, false);
-        range_track<STORE>(hmax, d0, d1, true);
+        range_track<STORE>(hmax, lo.x, lo.y);
+        range_track<STORE>(hmax, d0, d1);
         w.x = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.x, lo.y);
         w.y = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(d0, d1);
         reinterpret_cast<uint2 *>(out)[e] = w;
@@ -568,12 +556,8 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
         if (has1) reinterpret_cast<float2 *>(o1)[e] = make_float2(lo.y, hi.y);
       } else {
         const float d0 = __fsub_rn(hi.x, lo.x), d1 = __fsub_rn(hi.y, lo.y);
-        range_track<STORE>(hmax, lo.x, lo.x, false);
-        range_track<STORE>(hmax, d0, d0, true);
-        if (has1) {
-          range_track<STORE>(hmax, lo.y, lo.y, false);
-          range_track<STORE>(hmax, d1, d1, true);
-        }
+        range_track<STORE>(hmax, lo.x, d0);
+        if (has1) range_track<STORE>(hmax, lo.y, d1);
         reinterpret_cast<uint32_t *>(o0)[e] = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.x, d0);
         if (has1)
           reinterpret_cast<uint32_t *>(o1)[e] = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.y, d1);

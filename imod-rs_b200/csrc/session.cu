@@ -34,7 +34,7 @@ int cuda_fail(cudaError_t e, const char *what) {
 int device_error_status(int word) {
   if (word & 1) { set_error("a bounded device wait timed out"); return TG_ERR_TIMEOUT; }
   if (word & 4) {
-    set_error("a filtered projection or SIRT residual exceeds the FP16 staging range (|v| >= 16000); "
+    set_error("a filtered projection or SIRT residual exceeds the FP16 staging range (|v| >= 65520); "
               "the SIRT run diverges or the data need FP32/BF16 staging");
     return TG_ERR_RANGE;
   }

@@ -39,10 +39,9 @@ typedef enum {
   TG_ERR_NOT_READY = -9,    /* tg_server_wait: job still running */
   TG_ERR_NOT_FOUND = -10,   /* unknown job id */
   TG_ERR_CANCELLED = -11,   /* job dropped by tg_server_destroy before admission */
-  TG_ERR_RANGE = -12        /* FP16 staging: a filtered projection or SIRT residual exceeds what
-                               the FP16 staging holds (|v| >= 16000: up to four views are summed
-                               in half precision), e.g. a diverging SIRT run; the volume is
-                               not valid.  FP32/BF16 staging never report it. */
+  TG_ERR_RANGE = -12        /* FP16 staging: a filtered projection or SIRT residual exceeds the
+                               FP16 range (|v| >= 65520), e.g. a diverging SIRT run; the
+                               volume is not valid.  FP32/BF16 staging never report it. */
 } tg_status;
 
 /* Fill modes of apps/tilt/src/main.rs:122-128 */
@@ -170,17 +169,6 @@ size_t tg_session_device_bytes(tg_session *s);
  * reference (its wgpu queue is private); lets a host runtime order the work
  * with its own copies and timers. */
 int tg_session_set_stream(tg_session *s, void *cuda_stream);
-/* ---- Y slabs of one series on several GPUs (no counterpart in the reference,
- * which runs one process).  Without x-tilt or local alignment output slice iy
- * reads only projection row iy, so each rank can hold a slab of rows; the
- * per-view means of apps/tilt/src/main.rs:616-623 (the mean fill) still cover
- * whole views.  tg_session_view_sums returns the per-view f64 sums of the
- * uploaded rows (after --log), which the ranks add up (an all-reduce); each
- * rank then pins mean = (float)(sum / (nx * rows of the whole series)) with
- * tg_session_set_view_means (NULL: compute the means from the uploaded rows
- * again) before tg_reconstruct. */
-int tg_session_view_sums(tg_session *s, double *sums);
-int tg_session_set_view_means(tg_session *s, const float *means);
 /* Test hook of the bounded device waits (no counterpart in the reference).  The
  * pipelined back-projector's waits give up after wait_limit_us (0: the default
  * 2 s) and report TG_ERR_TIMEOUT through tg_synchronize.  skip_stage >= 0 makes
