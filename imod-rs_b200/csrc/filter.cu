@@ -385,21 +385,45 @@ __device__ __forceinline__ int swz(int e) { return e + (e >> 4); }
 __device__ __forceinline__ int swz_add(int swz_e, int off) { return swz_e + off + (off >> 4); }
 template <int N> __host__ __device__ constexpr int padded_len() { return N + N / 16; }
 
-// Radix of the pass that starts at span NS, for V values per thread: 8, 4 or 2
-// while N/NS allows it (and V is a multiple), the factor 3 of 3*2^k lengths last.
-template <int N, int NS, int V> struct PassRadix {
-  static constexpr int Q = N / NS;
-  static constexpr int R = (Q % 8 == 0 && V % 8 == 0) ? 8 : (Q % 4 == 0 && V % 4 == 0) ? 4
-                           : (Q % 2 == 0 && V % 2 == 0) ? 2 : 3;
-};
+// Radix of pass i of the forward transform, for V values per thread: 8, 4 or 2
+// while the remaining length allows it (and V is a multiple), the factor 3 of
+// 3*2^k lengths last.  The inverse takes the same radices in reverse order, so
+// its first butterflies combine exactly the values the forward's last
+// butterflies leave in each thread's registers (no exchange in between).
+__host__ __device__ constexpr int p2_radix(int N, int V, int i) {
+  int NS = 1, R = 1;
+  for (int p = 0; p <= i; ++p) {
+    const int Q = N / NS;
+    R = (Q % 8 == 0 && V % 8 == 0) ? 8 : (Q % 4 == 0 && V % 4 == 0) ? 4 : (Q % 2 == 0 && V % 2 == 0) ? 2 : 3;
+    NS *= R;
+  }
+  return R;
+}
+__host__ __device__ constexpr int p2_npass(int N, int V) {
+  int NS = 1, p = 0;
+  while (NS < N) NS *= p2_radix(N, V, p++);
+  return p;
+}
+// span (product of the earlier passes' radices) of pass i
+__host__ __device__ constexpr int p2_span(int N, int V, bool inv, int i) {
+  int NS = 1;
+  for (int p = 0; p < i; ++p) NS *= p2_radix(N, V, inv ? p2_npass(N, V) - 1 - p : p);
+  return NS;
+}
 
-// One Stockham pass over the values x[j] = X[t + j*N/V] held by thread t (V per
-// thread, so a pass of radix R is V/R butterflies per thread); writes to Y.
-template <int N, int V, int NS, bool INV>
-__device__ __forceinline__ void p2_pass(const float2 (&x)[V], int t, const float2 *__restrict__ tw, float2 *Y) {
+// Pass I of a transform over the values x[j] = X[t + j*N/V] held by thread t (V
+// per thread, so a pass of radix R is V/R butterflies per thread).  Writes the
+// results to Y, or (TOREG, the forward's last pass) back into x: that pass's
+// butterfly m reads and writes the positions t + (m + M*r)*T, which are x's own.
+template <int N, int V, bool INV, int I, bool TOREG>
+__device__ __forceinline__ void p2_pass(float2 (&x)[V], int t, const float2 *__restrict__ tw, float2 *Y) {
   constexpr int T = N / V;
-  constexpr int R = PassRadix<N, NS, V>::R;
+  constexpr int P = p2_npass(N, V);
+  constexpr int R = p2_radix(N, V, INV ? P - 1 - I : I);
+  constexpr int NS = p2_span(N, V, INV, I);
   constexpr int M = V / R;  // butterflies per thread
+  static_assert(V % R == 0, "values per thread must be a multiple of the radix");
+  static_assert(!TOREG || NS * R == N, "only a transform's last pass keeps its results in registers");
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     const int b = t + m * T;
@@ -416,27 +440,55 @@ __device__ __forceinline__ void p2_pass(const float2 (&x)[V], int t, const float
       }
     }
     dft_r<R, INV>(v);
-    const int sb = swz((b - k) * R + k);
+    if constexpr (TOREG) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) Y[swz_add(sb, r * NS)] = v[r];
+      for (int r = 0; r < R; ++r) x[m + M * r] = v[r];
+    } else {
+      const int base = (b - k) * R + k;
+      if constexpr ((NS & (NS - 1)) == 0 && R != 3) {  // power-of-two span and radix: offsets fold (swz_add)
+        const int sb = swz(base);
+#pragma unroll
+        for (int r = 0; r < R; ++r) Y[swz_add(sb, r * NS)] = v[r];
+      } else {  // the inverse of 3*2^k lengths: radix 3 first, then spans 3*2^j
+#pragma unroll
+        for (int r = 0; r < R; ++r) Y[swz(base + r * NS)] = v[r];
+      }
+    }
   }
 }
 
-// The passes of one transform; x holds the first pass's inputs.  Returns the
-// buffer holding the natural-order result.
-template <int N, int V, int NS, bool INV>
-__device__ __forceinline__ float2 *p2_fft(float2 (&x)[V], int t, const float2 *__restrict__ tw, float2 *A,
-                                         float2 *B) {
+// Forward transform from pass I on: x holds pass I's inputs; on return x holds
+// the spectrum values X[t + j*N/V].  Passes alternate between A and B, the
+// first one (I = 0) writing A.
+template <int N, int V, int I>
+__device__ __forceinline__ void p2_forward(float2 (&x)[V], int t, const float2 *__restrict__ tw, float2 *A,
+                                           float2 *B) {
   constexpr int T = N / V;
-  constexpr int R = PassRadix<N, NS, V>::R;
-  p2_pass<N, V, NS, INV>(x, t, tw, B);
-  __syncthreads();
-  if constexpr (NS * R < N) {
-#pragma unroll
-    for (int j = 0; j < V; ++j) x[j] = B[swz_add(swz(t), j * T)];
-    return p2_fft<N, V, NS * R, INV>(x, t, tw, B, A);
+  if constexpr (I == p2_npass(N, V) - 1) {
+    p2_pass<N, V, false, I, true>(x, t, tw, nullptr);
   } else {
-    return B;
+    p2_pass<N, V, false, I, false>(x, t, tw, A);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < V; ++j) x[j] = A[swz_add(swz(t), j * T)];
+    p2_forward<N, V, I + 1>(x, t, tw, B, A);
+  }
+}
+
+// Inverse transform from pass I on (x holds pass I's inputs, pass I writes A);
+// returns the buffer holding the natural-order result (after a barrier).
+template <int N, int V, int I>
+__device__ __forceinline__ float2 *p2_inverse(float2 (&x)[V], int t, const float2 *__restrict__ tw, float2 *A,
+                                              float2 *B) {
+  constexpr int T = N / V;
+  p2_pass<N, V, true, I, false>(x, t, tw, A);
+  __syncthreads();
+  if constexpr (I == p2_npass(N, V) - 1) {
+    return A;
+  } else {
+#pragma unroll
+    for (int j = 0; j < V; ++j) x[j] = A[swz_add(swz(t), j * T)];
+    return p2_inverse<N, V, I + 1>(x, t, tw, B, A);
   }
 }
 
@@ -462,105 +514,109 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
     }
     x[j] = make_float2(x0, x1);
   }
-  float2 *F = p2_fft<N, V, 1, false>(x, t, a.tw, A, B);
-  float2 *G = F == A ? B : A;
+  p2_forward<N, V, 0>(x, t, a.tw, A, B);
+  // x[j] = spectrum value t + j*T: x the radial weight, and for 2^k lengths the
+  // 1/n of the inverse too (a power of two: exact, and exact through the
+  // inverse's linear arithmetic, so the result is the one of scaling afterwards)
+  constexpr bool POW2 = (N & (N - 1)) == 0;
 #pragma unroll
-  for (int j = 0; j < V; ++j) {  // x the radial weight while loading the inverse's first pass
-    const int k = t + j * T;
-    const float w = __ldg(&a.weights[k]);
-    const float2 z = F[swz_add(swz(t), j * T)];
-    x[j] = make_float2(__fmul_rn(z.x, w), __fmul_rn(z.y, w));
+  for (int j = 0; j < V; ++j) {
+    float w = __ldg(&a.weights[t + j * T]);
+    if (POW2) w = __fmul_rn(w, a.inv_n);
+    x[j] = make_float2(__fmul_rn(x[j].x, w), __fmul_rn(x[j].y, w));
   }
-  // the inverse's first pass writes G (free since the forward's last barrier), not F,
-  // which other threads may still be reading above
-  const float2 *Rr = p2_fft<N, V, 1, true>(x, t, a.tw, F, G);
-  float2 *S = const_cast<float2 *>(Rr) == A ? B : A;
-  // scale by 1/n, then the cosine stretch of both rows at once (same source x)
+  // the forward's last exchange read buffer A (odd pass count) or B; the
+  // inverse's first pass writes the other one
+  constexpr int P = p2_npass(N, V);
+  const float2 *Rr = P % 2 == 0 ? p2_inverse<N, V, 0>(x, t, a.tw, B, A) : p2_inverse<N, V, 0>(x, t, a.tw, A, B);
   const float inv_n = a.inv_n;
-  const float stretch = a.stretch ? a.stretch[v] : 0.0f;
   auto sc = [&](int k) {
     const float2 z = Rr[swz(k)];
-    return make_float2(__fmul_rn(z.x, inv_n), __fmul_rn(z.y, inv_n));
+    return POW2 ? z : make_float2(__fmul_rn(z.x, inv_n), __fmul_rn(z.y, inv_n));
   };
-  if (stretch != 0.0f) {
-    const float center = __fdiv_rn((float)N, 2.0f);
-    for (int k = t; k < N; k += T) {
-      const float dx = __fsub_rn((float)k, center);
-      const float src_x = __fadd_rn(__fmul_rn(dx, stretch), center);
-      const float fl = floorf(src_x);
-      const int sx0 = fl < -1.0e9f ? -1000000000 : (int)fl;
-      const float frac = __fsub_rn(src_x, fl);
-      float2 o;
-      if (a.cubic && sx0 >= 1 && sx0 + 2 < N) {
-        const float2 p0 = sc(sx0 - 1), p1 = sc(sx0), p2 = sc(sx0 + 1), p3 = sc(sx0 + 2);
-        o = make_float2(cubic1d(p0.x, p1.x, p2.x, p3.x, frac), cubic1d(p0.y, p1.y, p2.y, p3.y, frac));
-      } else if (sx0 >= 0 && sx0 + 1 < N) {
-        const float2 p0 = sc(sx0), p1 = sc(sx0 + 1);
-        const float omf = __fsub_rn(1.0f, frac);
-        o = make_float2(__fadd_rn(__fmul_rn(p0.x, omf), __fmul_rn(p1.x, frac)),
-                        __fadd_rn(__fmul_rn(p0.y, omf), __fmul_rn(p1.y, frac)));
-      } else if (sx0 >= 0 && sx0 < N) {
-        o = sc(sx0);
-      } else {
-        o = make_float2(0.0f, 0.0f);
-      }
-      S[swz(k)] = o;
+  // final value of both rows at column k (0 <= k < N): the cosine stretch
+  // (main.rs:446-488) of the scaled inverse, or the scaled inverse itself
+  const float stretch = a.stretch ? a.stretch[v] : 0.0f;
+  const float center = __fdiv_rn((float)N, 2.0f);
+  auto fin = [&](int k) -> float2 {
+    if (stretch == 0.0f) return sc(k);
+    const float dx = __fsub_rn((float)k, center);
+    const float src_x = __fadd_rn(__fmul_rn(dx, stretch), center);
+    const float fl = floorf(src_x);
+    const int sx0 = fl < -1.0e9f ? -1000000000 : (int)fl;
+    const float frac = __fsub_rn(src_x, fl);
+    if (a.cubic && sx0 >= 1 && sx0 + 2 < N) {
+      const float2 p0 = sc(sx0 - 1), p1 = sc(sx0), p2 = sc(sx0 + 1), p3 = sc(sx0 + 2);
+      return make_float2(cubic1d(p0.x, p1.x, p2.x, p3.x, frac), cubic1d(p0.y, p1.y, p2.y, p3.y, frac));
     }
-  } else {
-    for (int k = t; k < N; k += T) S[swz(k)] = sc(k);
-  }
-  __syncthreads();
-  // pack into the staging format with the reference's fill rule (main.rs:386-406)
+    if (sx0 >= 0 && sx0 + 1 < N) {
+      const float2 p0 = sc(sx0), p1 = sc(sx0 + 1);
+      const float omf = __fsub_rn(1.0f, frac);
+      return make_float2(__fadd_rn(__fmul_rn(p0.x, omf), __fmul_rn(p1.x, frac)),
+                         __fadd_rn(__fmul_rn(p0.y, omf), __fmul_rn(p1.y, frac)));
+    }
+    if (sx0 >= 0 && sx0 < N) return sc(sx0);
+    return make_float2(0.0f, 0.0f);
+  };
+  // pack into the staging format with the reference's fill rule (main.rs:386-406):
+  // each thread takes two consecutive elements e, e+1 (PW is even), whose pairs
+  // need the final values at k, k+1, k+2 (k = e - padL), computed straight from
+  // the inverse (no second exchange)
   const float fillv = a.fill ? a.fill[v] : 0.0f;
-  float hmax = 0.0f;  // largest |value| packed into FP16 by this thread
-  auto pair = [&](int k, float2 &lo, float2 &hi) {  // (row[k], row[k+1]) of both rows, or the fill
-    if (k >= 0 && k + 1 < N) {
-      lo = S[swz(k)];
-      hi = S[swz(k + 1)];
-    } else {
-      float2 f;
-      if (a.fill_mode == TG_FILL_ZERO) f = make_float2(0.0f, 0.0f);
-      else if (a.fill_mode == TG_FILL_EDGE) f = k < 0 ? S[swz(0)] : S[swz(N - 1)];
-      else f = make_float2(fillv, fillv);
-      lo = hi = f;
-    }
+  auto fill = [&](int k) -> float2 {
+    if (a.fill_mode == TG_FILL_ZERO) return make_float2(0.0f, 0.0f);
+    if (a.fill_mode == TG_FILL_EDGE) return fin(k < 0 ? 0 : N - 1);
+    return make_float2(fillv, fillv);
   };
-  if (FMT == FMT_ROWPAIR) {
-    uint8_t *out = reinterpret_cast<uint8_t *>(a.out) +
-                   ((size_t)v * a.rows_alloc + jp) * (size_t)a.PW * (STORE == TG_STORE_FP32 ? 16 : 8);
-    for (int e = t; e < a.PW; e += T) {
-      float2 lo, hi;
-      pair(e - a.padL, lo, hi);
-      if (!has1) lo.y = hi.y = 0.0f;
+  float hmax = 0.0f;  // largest |value| packed into FP16 by this thread
+  const size_t row0 = (size_t)v * a.rows_alloc;
+  for (int e = 2 * t; e < a.PW; e += 2 * T) {
+    const int k = e - a.padL;
+    float2 f0 = make_float2(0.0f, 0.0f), f1 = f0, f2 = f0;
+    if (k >= 0 && k < N) f0 = fin(k);
+    if (k + 1 >= 0 && k + 1 < N) f1 = fin(k + 1);
+    if (k + 2 >= 0 && k + 2 < N) f2 = fin(k + 2);
+    float2 lo0 = f0, hi0 = f1, lo1 = f1, hi1 = f2;  // (row[k], row[k+1]) and (row[k+1], row[k+2])
+    if (!(k >= 0 && k + 1 < N)) lo0 = hi0 = fill(k);
+    if (!(k + 1 >= 0 && k + 2 < N)) lo1 = hi1 = fill(k + 1);
+    if (!has1) lo0.y = hi0.y = lo1.y = hi1.y = 0.0f;
+    if (FMT == FMT_ROWPAIR) {
+      uint8_t *out = reinterpret_cast<uint8_t *>(a.out) +
+                     (row0 + jp) * (size_t)a.PW * (STORE == TG_STORE_FP32 ? 16 : 8);
       if (STORE == TG_STORE_FP32) {
-        reinterpret_cast<float4 *>(out)[e] = make_float4(lo.x, lo.y, hi.x, hi.y);
+        float4 *o = reinterpret_cast<float4 *>(out) + e;
+        o[0] = make_float4(lo0.x, lo0.y, hi0.x, hi0.y);
+        o[1] = make_float4(lo1.x, lo1.y, hi1.x, hi1.y);
       } else {
-        uint2 w;
-        const float d0 = __fsub_rn(hi.x, lo.x), d1 = __fsub_rn(hi.y, lo.y);
-        range_track<STORE>(hmax, lo.x, lo.y);
-        range_track<STORE>(hmax, d0, d1);
-        w.x = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.x, lo.y);
-        w.y = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(d0, d1);
-        reinterpret_cast<uint2 *>(out)[e] = w;
+        using PK = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>;
+        const float d0x = __fsub_rn(hi0.x, lo0.x), d0y = __fsub_rn(hi0.y, lo0.y);
+        const float d1x = __fsub_rn(hi1.x, lo1.x), d1y = __fsub_rn(hi1.y, lo1.y);
+        range_track<STORE>(hmax, lo0.x, lo0.y);
+        range_track<STORE>(hmax, lo1.x, lo1.y);
+        range_track<STORE>(hmax, d0x, d0y);
+        range_track<STORE>(hmax, d1x, d1y);
+        reinterpret_cast<uint4 *>(out)[e >> 1] =
+            make_uint4(PK::h2(lo0.x, lo0.y), PK::h2(d0x, d0y), PK::h2(lo1.x, lo1.y), PK::h2(d1x, d1y));
       }
-    }
-  } else {
-    const int eb = STORE == TG_STORE_FP32 ? 8 : 4;
-    uint8_t *o0 = reinterpret_cast<uint8_t *>(a.out) + ((size_t)v * a.rows_alloc + r0) * (size_t)a.PW * eb;
-    uint8_t *o1 = o0 + (size_t)a.PW * eb;
-    for (int e = t; e < a.PW; e += T) {
-      float2 lo, hi;
-      pair(e - a.padL, lo, hi);
+    } else {
+      const int eb = STORE == TG_STORE_FP32 ? 8 : 4;
+      uint8_t *o0 = reinterpret_cast<uint8_t *>(a.out) + (row0 + r0) * (size_t)a.PW * eb;
+      uint8_t *o1 = o0 + (size_t)a.PW * eb;
       if (STORE == TG_STORE_FP32) {
-        reinterpret_cast<float2 *>(o0)[e] = make_float2(lo.x, hi.x);
-        if (has1) reinterpret_cast<float2 *>(o1)[e] = make_float2(lo.y, hi.y);
+        reinterpret_cast<float4 *>(o0)[e >> 1] = make_float4(lo0.x, hi0.x, lo1.x, hi1.x);
+        if (has1) reinterpret_cast<float4 *>(o1)[e >> 1] = make_float4(lo0.y, hi0.y, lo1.y, hi1.y);
       } else {
-        const float d0 = __fsub_rn(hi.x, lo.x), d1 = __fsub_rn(hi.y, lo.y);
-        range_track<STORE>(hmax, lo.x, d0);
-        if (has1) range_track<STORE>(hmax, lo.y, d1);
-        reinterpret_cast<uint32_t *>(o0)[e] = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.x, d0);
-        if (has1)
-          reinterpret_cast<uint32_t *>(o1)[e] = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>::h2(lo.y, d1);
+        using PK = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>;
+        const float d0x = __fsub_rn(hi0.x, lo0.x), d0y = __fsub_rn(hi0.y, lo0.y);
+        const float d1x = __fsub_rn(hi1.x, lo1.x), d1y = __fsub_rn(hi1.y, lo1.y);
+        range_track<STORE>(hmax, lo0.x, lo1.x);
+        range_track<STORE>(hmax, d0x, d1x);
+        if (has1) {
+          range_track<STORE>(hmax, lo0.y, lo1.y);
+          range_track<STORE>(hmax, d0y, d1y);
+        }
+        reinterpret_cast<uint2 *>(o0)[e >> 1] = make_uint2(PK::h2(lo0.x, d0x), PK::h2(lo1.x, d1x));
+        if (has1) reinterpret_cast<uint2 *>(o1)[e >> 1] = make_uint2(PK::h2(lo0.y, d0y), PK::h2(lo1.y, d1y));
       }
     }
   }
