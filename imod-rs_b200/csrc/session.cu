@@ -781,6 +781,40 @@ int tg_set_projections_device(tg_session *s, const float *dev, size_t n) {
   return TG_OK;
 }
 
+namespace tg {
+// n SIRT iterations (main.rs:919-975) on the session's stream: reprojection,
+// residual R-weighting, relaxed back-projection update; one CUDA graph per
+// iteration, captured on first use, when the session uses graphs
+int sirt_iterations(tg_session *s, int n) {
+  auto one_iter = [&]() -> int {
+    s->iter_launches = launch_reproject(fp_args(s), s->st) + 1 + bp_launch_count(s);
+    launch_filter(filter_args(s, true), s->st);
+    return launch_bp(s, 2, nullptr);
+  };
+  if (n <= 0) return TG_OK;
+  if (s->o.use_graphs) {
+    if (!s->sirt_exec) {
+      cudaGraph_t graph;
+      TG_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeRelaxed));
+      int r2 = one_iter();
+      cudaError_t ec = cudaStreamEndCapture(s->st, &graph);
+      if (r2 != TG_OK) return r2;
+      if (ec != cudaSuccess) return cuda_fail(ec, "cudaStreamEndCapture");
+      ec = cudaGraphInstantiate(&s->sirt_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ec != cudaSuccess) return cuda_fail(ec, "cudaGraphInstantiate");
+    }
+    for (int it = 0; it < n; ++it) TG_CUDA(cudaGraphLaunch(s->sirt_exec, s->st));
+  } else {
+    for (int it = 0; it < n; ++it) {
+      const int rc = one_iter();
+      if (rc != TG_OK) return rc;
+    }
+  }
+  return TG_OK;
+}
+}  // namespace tg
+
 int tg_reconstruct(tg_session *s) {
   if (!s) return TG_ERR_INVALID_ARG;
   if (!s->uploaded) { set_error("no projections uploaded"); return TG_ERR_INVALID_ARG; }
@@ -790,6 +824,7 @@ int tg_reconstruct(tg_session *s) {
   if (s->variant < 0 && (rc = autotune(s)) != TG_OK) return rc;
   const int iters = sirt_iters(s);
   s->timed = false;
+  s->sirt_done = -1;  // closes a SIRT run in steps
   TG_CUDA(cudaEventRecord(s->ev[0], s->st));
   {
     NvtxRange r("tg.filter");
@@ -806,28 +841,7 @@ int tg_reconstruct(tg_session *s) {
   TG_CUDA(cudaEventRecord(s->ev[2], s->st));
   if (iters > 0) {
     NvtxRange r("tg.sirt");
-    auto one_iter = [&]() -> int {
-      s->iter_launches = launch_reproject(fp_args(s), s->st) + 1 + bp_launch_count(s);
-      launch_filter(filter_args(s, true), s->st);
-      return launch_bp(s, 2, nullptr);
-    };
-    if (s->o.use_graphs) {
-      if (!s->sirt_exec) {
-        cudaGraph_t graph;
-        TG_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeRelaxed));
-        int r2 = one_iter();
-        cudaError_t ec = cudaStreamEndCapture(s->st, &graph);
-        if (r2 != TG_OK) return r2;
-        if (ec != cudaSuccess) return cuda_fail(ec, "cudaStreamEndCapture");
-        ec = cudaGraphInstantiate(&s->sirt_exec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (ec != cudaSuccess) return cuda_fail(ec, "cudaGraphInstantiate");
-      }
-      for (int it = 0; it < iters; ++it) TG_CUDA(cudaGraphLaunch(s->sirt_exec, s->st));
-    } else {
-      for (int it = 0; it < iters; ++it)
-        if ((rc = one_iter()) != TG_OK) return rc;
-    }
+    if ((rc = sirt_iterations(s, iters)) != TG_OK) return rc;
     launches += s->iter_launches * iters;  // counted when the iteration was issued or captured
   }
   TG_CUDA(cudaEventRecord(s->ev[3], s->st));
@@ -841,6 +855,80 @@ int tg_reconstruct(tg_session *s) {
   s->info.updates = (double)s->onx * s->onz * s->ny * s->nviews * (1.0 + 2.0 * iters);
   s->info.kernel_launches = launches;
   s->timed = true;
+  return TG_OK;
+}
+
+int tg_sirt_begin(tg_session *s) {
+  if (!s) return TG_ERR_INVALID_ARG;
+  if (!s->uploaded) { set_error("no projections uploaded"); return TG_ERR_INVALID_ARG; }
+  if (sirt_iters(s) <= 0) { set_error("the session runs no SIRT iterations"); return TG_ERR_INVALID_ARG; }
+  TG_CUDA(cudaSetDevice(s->dev));
+  (void)cudaGetLastError();
+  int rc, launches = 0;
+  if (s->variant < 0 && (rc = autotune(s)) != TG_OK) return rc;
+  s->timed = false;
+  s->sirt_done = -1;
+  if ((rc = stage_front(s, &launches)) != TG_OK) return rc;
+  if ((rc = launch_bp(s, first_mode(s), nullptr)) != TG_OK) return rc;  // mode 1: raw sums, no statistics
+  TG_CUDA(cudaGetLastError());
+  s->sirt_done = 0;
+  return TG_OK;
+}
+
+int tg_sirt_iterate(tg_session *s, int32_t n) {
+  if (!s || n < 0) return TG_ERR_INVALID_ARG;
+  if (s->sirt_done < 0) { set_error("no SIRT run open (tg_sirt_begin or tg_sirt_restore first)"); return TG_ERR_INVALID_ARG; }
+  if (s->sirt_done + n > sirt_iters(s)) {
+    set_error("more SIRT iterations than the session's sirt_iters");
+    return TG_ERR_INVALID_ARG;
+  }
+  TG_CUDA(cudaSetDevice(s->dev));
+  const int rc = sirt_iterations(s, n);
+  if (rc != TG_OK) return rc;
+  s->sirt_done += n;
+  return TG_OK;
+}
+
+int tg_sirt_end(tg_session *s) {
+  if (!s) return TG_ERR_INVALID_ARG;
+  if (s->sirt_done < 0) { set_error("no SIRT run open"); return TG_ERR_INVALID_ARG; }
+  TG_CUDA(cudaSetDevice(s->dev));
+  int launches = 0;
+  const int rc = stage_finish(s, first_mode(s), 0, &launches);
+  if (rc != TG_OK) return rc;
+  s->sirt_done = -1;
+  return TG_OK;
+}
+
+int tg_sirt_save(tg_session *s, float *host_volume, int32_t *iterations_done) {
+  if (!s || !host_volume) return TG_ERR_INVALID_ARG;
+  if (s->sirt_done < 0) { set_error("no SIRT run open"); return TG_ERR_INVALID_ARG; }
+  const int rc = tg_synchronize(s);
+  if (rc != TG_OK) return rc;
+  TG_CUDA(cudaMemcpy(host_volume, s->d_vol, (size_t)s->onx * s->onz * s->ny * 4, cudaMemcpyDeviceToHost));
+  if (iterations_done) *iterations_done = s->sirt_done;
+  return TG_OK;
+}
+
+int tg_sirt_restore(tg_session *s, const float *host_volume, int32_t iterations_done) {
+  if (!s || !host_volume || iterations_done < 0) return TG_ERR_INVALID_ARG;
+  if (!s->uploaded) { set_error("no projections uploaded"); return TG_ERR_INVALID_ARG; }
+  if (sirt_iters(s) <= 0 || iterations_done > sirt_iters(s)) {
+    set_error("iteration count outside the session's SIRT run");
+    return TG_ERR_INVALID_ARG;
+  }
+  TG_CUDA(cudaSetDevice(s->dev));
+  (void)cudaGetLastError();
+  int rc;
+  if (s->variant < 0 && (rc = autotune(s)) != TG_OK) return rc;
+  s->timed = false;
+  // the log and the per-view means the iterations read (main.rs:608-623)
+  launch_log_means(s->d_raw, s->d_logd, s->nx * s->ny, s->nz, s->d_mpart, s->means_pinned ? nullptr : s->d_means,
+                   s->st);
+  TG_CUDA(cudaMemcpyAsync(s->d_vol, host_volume, (size_t)s->onx * s->onz * s->ny * 4, cudaMemcpyHostToDevice,
+                          s->st));
+  TG_CUDA(cudaStreamSynchronize(s->st));  // the pageable source may be reused on return
+  s->sirt_done = iterations_done;
   return TG_OK;
 }
 

@@ -69,6 +69,7 @@ struct tg_session {  // one tilt series resident on a device
   unsigned long long wait_limit_ns = 2000000000ull;
   int fault_skip_stage = -1;
   int iter_launches = 0;  // kernels of one SIRT iteration
+  int sirt_done = -1;     // SIRT in steps: iterations done since tg_sirt_begin/restore (-1: none open)
   float cx = 0, cz = 0, ocx = 0, inv_n = 0;
   cudaMemPool_t pool = nullptr;  // stream-ordered allocations (server sessions)
   bool dry = false, fail_alloc = false;

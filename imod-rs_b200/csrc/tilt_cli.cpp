@@ -54,6 +54,8 @@ struct Args {
   int device = 0;
   int mode = 2;  // output MRC mode: 2 (float, the reference's) or 12 (half)
   long io_chunk_kb = 128 * 1024;  // pinned staging chunk of the read and write pipelines
+  std::string checkpoint, resume;  // SIRT state files (MRC, iteration count in the first label)
+  long checkpoint_every = 10;
 };
 
 void usage(FILE *f) {
@@ -92,6 +94,10 @@ void usage(FILE *f) {
           "      --mode <2|12>                Output MRC mode: 2 float, 12 half (addition) [default: 2]\n"
           "      --io-chunk-kb <N>            Staging chunk of the overlapped read/write (addition)\n"
           "                                   [default: 131072]\n"
+          "      --checkpoint <FILE>          Write the SIRT state (raw volume, iteration count) to\n"
+          "                                   FILE every --checkpoint-every iterations (addition)\n"
+          "      --checkpoint-every <K>       [default: 10]\n"
+          "      --resume <FILE>              Continue SIRT from a --checkpoint file (addition)\n"
           "  -h, --help                       Print help\n\n"
           "PIP-style aliases (additions): -InputProjections -OutputFile -TILTFILE -THICKNESS\n"
           "  -WIDTH -RADIAL -SIRTIterations -LOG -SCALE <add,mult> -FakeSIRTiterations\n"
@@ -203,6 +209,9 @@ Args parse(int argc, char **argv) {
     else if (name == "storage") a.storage = lower(val);
     else if (name == "device") a.device = (int)parse_int(val, "--device", false);
     else if (name == "io-chunk-kb") a.io_chunk_kb = std::max(1L, parse_int(val, "--io-chunk-kb", false));
+    else if (name == "checkpoint") a.checkpoint = val;
+    else if (name == "resume") a.resume = val;
+    else if (name == "checkpoint-every") a.checkpoint_every = std::max(1L, parse_int(val, "--checkpoint-every", false));
     else if (name == "mode") {
       a.mode = (int)parse_int(val, "--mode", false);
       if (a.mode != 2 && a.mode != 12) clap_error("invalid value '" + val + "' for '--mode': 2 or 12");
@@ -221,6 +230,97 @@ Args parse(int argc, char **argv) {
   if (!has_tlt) missing += "\n  --tilt-file <TILT_FILE>";
   if (!missing.empty()) clap_error("the following required arguments were not provided:" + missing);
   return a;
+}
+
+// First label of a checkpoint file: the iteration count and the run's total.
+constexpr const char *CKPT_LABEL = "tiltgpu SIRT state: iterations ";
+constexpr int CKPT_FILE_ERROR = 1;  // run_sirt_steps: a checkpoint file could not be read or written
+
+// The raw SIRT volume ([y][out_nz][out_nx], before the output transform) as an
+// MRC float volume of out_ny sections; written to FILE.tmp, then renamed, so an
+// interrupted write leaves the previous checkpoint in place.
+bool write_checkpoint(const std::string &path, const std::vector<float> &vol, int out_nx, int out_nz, int out_ny,
+                      int done, int total, std::string *err) {
+  mrc::Header h = mrc::Header::make(out_nx, out_nz, out_ny, mrc::FLOAT);
+  h.add_label(std::string(CKPT_LABEL) + std::to_string(done) + " of " + std::to_string(total));
+  const std::string tmp = path + ".tmp";
+  {
+    mrc::Writer w;
+    if (!w.create(tmp, h, err)) return false;
+    const size_t slice = (size_t)out_nx * out_nz;
+    for (int y = 0; y < out_ny; ++y)
+      if (!w.write_slice_f32(vol.data() + (size_t)y * slice, slice, err)) return false;
+    if (!w.finish(0.0f, 0.0f, 0.0f, err)) return false;
+  }
+  if (std::rename(tmp.c_str(), path.c_str()) != 0) {
+    *err = "cannot rename " + tmp + " to " + path;
+    return false;
+  }
+  return true;
+}
+
+bool read_checkpoint(const std::string &path, std::vector<float> &vol, int out_nx, int out_nz, int out_ny,
+                     int *done, std::string *err) {
+  mrc::Reader r;
+  if (!r.open(path, err)) return false;
+  const mrc::Header &h = r.header();
+  const std::string lab = h.nlabl > 0 ? h.label(0) : std::string();
+  if (lab.rfind(CKPT_LABEL, 0) != 0) {
+    *err = path + " is not a SIRT checkpoint of this program";
+    return false;
+  }
+  *done = atoi(lab.c_str() + strlen(CKPT_LABEL));
+  if (h.nx != out_nx || h.ny != out_nz || h.nz != out_ny || h.mode != mrc::FLOAT) {
+    *err = path + ": volume size or mode does not match this reconstruction";
+    return false;
+  }
+  vol.resize((size_t)out_nx * out_nz * out_ny);
+  std::vector<float> sl;
+  const size_t slice = (size_t)out_nx * out_nz;
+  for (int y = 0; y < out_ny; ++y) {
+    if (!r.read_slice_f32(y, sl, err) || sl.size() != slice) return false;
+    std::copy(sl.begin(), sl.end(), vol.begin() + (size_t)y * slice);
+  }
+  return true;
+}
+
+// SIRT in steps (tg_sirt_*): from the WBP start or a --resume state, iterations in
+// groups of --checkpoint-every, the state written after each group that leaves
+// iterations to run, then the output stage.  Same volume as tg_reconstruct.
+int run_sirt_steps(tg_session *s, const Args &args, int out_nx, int out_nz, int out_ny) {
+  int rc, done = 0;
+  const int total = (int)args.sirt;
+  std::vector<float> vol;
+  std::string err;
+  if (!args.resume.empty()) {
+    if (!read_checkpoint(args.resume, vol, out_nx, out_nz, out_ny, &done, &err)) {
+      fprintf(stderr, "Error: %s\n", err.c_str());
+      return CKPT_FILE_ERROR;
+    }
+    if ((rc = tg_sirt_restore(s, vol.data(), done)) != TG_OK) return rc;
+    fprintf(stderr, "tilt: resuming SIRT after %d of %d iterations\n", done, total);
+  } else if ((rc = tg_sirt_begin(s)) != TG_OK) {
+    return rc;
+  }
+  const int every = args.checkpoint.empty() ? total : (int)args.checkpoint_every;
+  while (done < total) {
+    const int n = std::min(every, total - done);
+    if ((rc = tg_sirt_iterate(s, n)) != TG_OK) return rc;
+    done += n;
+    if (!args.checkpoint.empty() && done < total) {
+      vol.resize((size_t)out_nx * out_nz * out_ny);
+      int32_t d = 0;
+      if ((rc = tg_sirt_save(s, vol.data(), &d)) != TG_OK) return rc;
+      if (!write_checkpoint(args.checkpoint, vol, out_nx, out_nz, out_ny, d, total, &err)) {
+        fprintf(stderr, "Error: %s\n", err.c_str());
+        return CKPT_FILE_ERROR;
+      }
+      fprintf(stderr, "tilt: SIRT state after %d of %d iterations written to %s\n", d, total,
+              args.checkpoint.c_str());
+    }
+  }
+  if ((rc = tg_sirt_end(s)) != TG_OK) return rc;
+  return tg_synchronize(s);
 }
 
 }  // namespace
@@ -408,7 +508,16 @@ int main(int argc, char **argv) {
     }
   }
   const auto t_rec0 = clk::now();
-  if ((rc = tg_reconstruct(s)) != TG_OK || (rc = tg_synchronize(s)) != TG_OK) return fail(rc);
+  const bool steps = args.sirt > 0 && !args.gpu && (!args.checkpoint.empty() || !args.resume.empty());
+  if (!steps) {
+    if ((rc = tg_reconstruct(s)) != TG_OK || (rc = tg_synchronize(s)) != TG_OK) return fail(rc);
+  } else if ((rc = run_sirt_steps(s, args, out_nx, out_nz, out_ny)) != TG_OK) {
+    if (rc == CKPT_FILE_ERROR) {  // reported already
+      tg_session_destroy(s);
+      return 1;
+    }
+    return fail(rc);
+  }
   const auto t_rec1 = clk::now();
   uint8_t hin[1024], hout[1024];  // main.rs:710-717
   h.to_bytes(hin, false);

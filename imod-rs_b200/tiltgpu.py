@@ -160,6 +160,11 @@ EXPORTS = {
     "tg_upload_sections": (C.c_int, [_P, _i32, _i32, _P]),
     "tg_session_inject_wait_fault": (C.c_int, [_P, _i32, C.c_uint32]),
     "tg_session_view_sums": (C.c_int, [_P, _P]),
+    "tg_sirt_begin": (C.c_int, [_P]),
+    "tg_sirt_iterate": (C.c_int, [_P, _i32]),
+    "tg_sirt_end": (C.c_int, [_P]),
+    "tg_sirt_save": (C.c_int, [_P, _P, C.POINTER(_i32)]),
+    "tg_sirt_restore": (C.c_int, [_P, _P, _i32]),
     "tg_session_set_view_means": (C.c_int, [_P, _P]),
     "tg_download_slices_f16_async": (C.c_int, [_P, _i32, _i32, _P]),
     "tg_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_P)]),
@@ -339,6 +344,31 @@ class Session:
         """Pins the mean fill values (whole-series means of a slab); None: compute them again."""
         m = None if means is None else _f32(means)
         check(lib().tg_session_set_view_means(self.h, _ptr(m)))
+
+    # SIRT in steps with checkpoints (tg_sirt_*)
+    def sirt_begin(self):
+        """Log, means, R-weighting and the WBP start; 0 SIRT iterations done."""
+        check(lib().tg_sirt_begin(self.h))
+
+    def sirt_iterate(self, n: int):
+        check(lib().tg_sirt_iterate(self.h, int(n)))
+
+    def sirt_end(self):
+        """Output stage: the volume and statistics of tg_reconstruct with the iterations run."""
+        check(lib().tg_sirt_end(self.h))
+
+    def sirt_save(self):
+        """(raw SIRT volume [y][z][x], iterations done), synchronising."""
+        vol = np.empty(self.out_shape, np.float32)
+        done = _i32(0)
+        check(lib().tg_sirt_save(self.h, _ptr(vol), C.byref(done)))
+        return vol, int(done.value)
+
+    def sirt_restore(self, vol, iterations_done: int):
+        v = np.ascontiguousarray(vol, np.float32)
+        if v.shape != tuple(self.out_shape):
+            raise ValueError(f"volume shape {v.shape} != {tuple(self.out_shape)}")
+        check(lib().tg_sirt_restore(self.h, _ptr(v), int(iterations_done)))
 
     def inject_wait_fault(self, skip_stage=-1, wait_limit_us=0):
         """Test hook: the back-projector's producer leaves out one pipeline stage and

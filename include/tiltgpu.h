@@ -178,6 +178,27 @@ int tg_session_set_stream(tg_session *s, void *cuda_stream);
  * restore normal operation).  TG_ERR_UNSUPPORTED for sessions that do not use
  * that back-projector (local alignment, per-view x-tilts). */
 int tg_session_inject_wait_fault(tg_session *s, int32_t skip_stage, uint32_t wait_limit_us);
+/* ---- SIRT in steps, with checkpoints (no counterpart in the reference, whose
+ * SIRT loop apps/tilt/src/main.rs:919-975 runs to the end in one process) ----
+ * tg_sirt_begin runs what tg_reconstruct runs before the first SIRT iteration
+ * (log, means, R-weighting and the WBP start: iteration count 0);
+ * tg_sirt_iterate runs n more iterations (at most the session's sirt_iters in
+ * all); tg_sirt_end runs the output stage (fake SIRT, output transform,
+ * statistics), after which the volume and statistics are those of
+ * tg_reconstruct with the iterations run so far.  Between them, tg_sirt_save
+ * copies the raw SIRT volume ([y][out_nz][out_nx] f32, before the output
+ * transform) and the iteration count to the host (synchronising), and
+ * tg_sirt_restore puts them back into a session with the same geometry and
+ * options whose projections are uploaded (it recomputes the log and means),
+ * so that iterating on continues the saved run: begin, k iterations, save,
+ * then restore, n - k iterations, end gives tg_reconstruct's n-iteration result
+ * bit for bit.  TG_ERR_INVALID_ARG without SIRT (sirt_iters 0, --gpu), out of
+ * order, or with more iterations than sirt_iters. */
+int tg_sirt_begin(tg_session *s);
+int tg_sirt_iterate(tg_session *s, int32_t n);
+int tg_sirt_end(tg_session *s);
+int tg_sirt_save(tg_session *s, float *host_volume, int32_t *iterations_done);
+int tg_sirt_restore(tg_session *s, const float *host_volume, int32_t iterations_done);
 int tg_session_destroy(tg_session *s);
 
 /* ---- Batched reconstruction of many series (no counterpart in the reference,

@@ -89,3 +89,12 @@ def test_mode_flag_accepts_2_and_12_only():
     r = run("-i", "a", "-o", "b", "-t", "c", "--mode", "4")
     assert r.returncode == 2 and "--mode" in r.stderr
     assert "--mode" in run("--help").stdout and "--io-chunk-kb" in run("--help").stdout
+
+
+def test_checkpoint_flags():
+    h = run("--help").stdout
+    assert "--checkpoint <FILE>" in h and "--checkpoint-every" in h and "--resume <FILE>" in h
+    r = run("-i", "a", "-o", "b", "-t", "c", "--checkpoint-every", "x")
+    assert r.returncode == 2 and "--checkpoint-every" in r.stderr
+    r = run("-i", "a", "-o", "b", "-t", "c", "--resume")
+    assert r.returncode == 2 and "a value is required for '--resume'" in r.stderr
