@@ -49,19 +49,26 @@ __device__ __forceinline__ float log_sample(float x) { return (float)log10((doub
 // samples against the FP64 log10 found at most 2^-47.6), so z rounded to float
 // is the correctly rounded log unless z lies within 2^-40 |z| of a midpoint
 // between floats; those samples (about 2 in 10^5), x = 1 (z = 0) and infinite
-// x take log_sample.  lt holds (inv_j, -ln inv_j) in double.
-__device__ __forceinline__ float log_sample_fast(float x, const double2 *lt) {
+// x take log_sample.  The table (shared memory) holds inv_j as float and
+// -ln inv_j as double, in separate arrays: neighbouring centres sit in
+// different banks, so the lanes of a warp (similar values, nearby centres)
+// rarely conflict.
+struct LogTable {
+  float inv[257];
+  double nl[257];
+};
+__device__ __forceinline__ float log_sample_fast(float x, const LogTable &lt) {
   x = fmaxf(x, 0.001f);
   const int ix = __float_as_int(x);
   const int e = (ix - 0x3f400000) >> 23;
   const int mb = ix - (e << 23);
-  const double2 c = lt[(mb - 0x3f400000 + 0x4000) >> 15];
-  const double r = __fma_rn((double)__int_as_float(mb), c.x, -1.0);
+  const int j = (mb - 0x3f400000 + 0x4000) >> 15;
+  const double r = __fma_rn((double)__int_as_float(mb), (double)lt.inv[j], -1.0);
   double p = __fma_rn(r, 0.2, -0.25);
   p = __fma_rn(r, p, 1.0 / 3.0);
   p = __fma_rn(r, p, -0.5);
   p = __fma_rn(r, p, 1.0);
-  const double z = __dmul_rn(__dadd_rn(__fma_rn((double)e, 0.693147180559945309417232121458176568, c.y),
+  const double z = __dmul_rn(__dadd_rn(__fma_rn((double)e, 0.693147180559945309417232121458176568, lt.nl[j]),
                                        __dmul_rn(r, p)),
                              0.434294481903251827651128918916605082);  // ln 2, log10 e
   const float f = __double2float_rn(z);
@@ -74,20 +81,27 @@ __device__ __forceinline__ float log_sample_fast(float x, const double2 *lt) {
   return log_sample(x);
 }
 
-// (inv_j, -ln inv_j) for the 257 centres of log_sample_fast, into shared memory
-__device__ __forceinline__ void log_table(double2 *lt) {
+// the 257 centres' (inv_j, -ln inv_j) of log_sample_fast
+__device__ __forceinline__ void log_table(LogTable &lt) {
   for (int i = threadIdx.x; i < 257; i += blockDim.x) {
     const float inv = __frcp_rn(__int_as_float(0x3f400000 + (i << 15)));
-    lt[i] = make_double2((double)inv, -log((double)inv));
+    lt.inv[i] = inv;
+    lt.nl[i] = -log((double)inv);
   }
   __syncthreads();
+}
+
+template <bool LOG> __device__ __forceinline__ float4 log4(float4 x, const LogTable &lt) {
+  return LOG ? make_float4(log_sample_fast(x.x, lt), log_sample_fast(x.y, lt), log_sample_fast(x.z, lt),
+                           log_sample_fast(x.w, lt))
+             : x;
 }
 
 template <bool LOG>
 __global__ void __launch_bounds__(256) log_sum_kernel(const float *__restrict__ raw, float *__restrict__ logd,
                                                       long npix, double *partials) {
   const int v = blockIdx.y, c = blockIdx.x;
-  __shared__ double2 lt[LOG ? 257 : 1];
+  __shared__ LogTable lt;
   if (LOG) log_table(lt);
   const size_t base = (size_t)v * npix;
   const long c0 = npix * c / MEAN_CH, c1 = npix * (c + 1) / MEAN_CH;
@@ -103,18 +117,27 @@ __global__ void __launch_bounds__(256) log_sum_kernel(const float *__restrict__ 
   }
   const float4 *r4 = reinterpret_cast<const float4 *>(raw + base + a0);
   float4 *l4 = LOG ? reinterpret_cast<float4 *>(logd + base + a0) : nullptr;
-  for (long i = threadIdx.x; i < (a1 - a0) / 4; i += blockDim.x) {
-    float4 x = __ldcs(r4 + i);
+  const long n4 = (a1 - a0) / 4;
+  long i = threadIdx.x;
+  // two 16-byte loads in flight per thread (the loop is latency-bound on HBM otherwise)
+  for (; i + (long)blockDim.x < n4; i += 2L * blockDim.x) {
+    const float4 u = __ldcs(r4 + i), w = __ldcs(r4 + i + blockDim.x);
+    const float4 x = log4<LOG>(u, lt), y = log4<LOG>(w, lt);
     if (LOG) {
-      x = make_float4(log_sample_fast(x.x, lt), log_sample_fast(x.y, lt), log_sample_fast(x.z, lt),
-                      log_sample_fast(x.w, lt));
       l4[i] = x;
+      l4[i + blockDim.x] = y;
     }
     s += ((double)x.x + (double)x.y) + ((double)x.z + (double)x.w);
+    s += ((double)y.x + (double)y.y) + ((double)y.z + (double)y.w);
   }
-  for (long i = a1 + threadIdx.x; i < c1; i += blockDim.x) {
-    float x = raw[base + i];
-    if (LOG) logd[base + i] = x = log_sample_fast(x, lt);
+  if (i < n4) {
+    const float4 x = log4<LOG>(__ldcs(r4 + i), lt);
+    if (LOG) l4[i] = x;
+    s += ((double)x.x + (double)x.y) + ((double)x.z + (double)x.w);
+  }
+  for (long k = a1 + threadIdx.x; k < c1; k += blockDim.x) {
+    float x = raw[base + k];
+    if (LOG) logd[base + k] = x = log_sample_fast(x, lt);
     s += (double)x;
   }
   __shared__ double red[8];
@@ -436,9 +459,7 @@ template <int N> __host__ __device__ constexpr int padded_len() { return N + N /
 
 // Radix of pass i of the forward transform, for V values per thread: 8, 4 or 2
 // while the remaining length allows it (and V is a multiple), the factor 3 of
-// 3*2^k lengths last.  The inverse takes the same radices in reverse order, so
-// its first butterflies combine exactly the values the forward's last
-// butterflies leave in each thread's registers (no exchange in between).
+// 3*2^k lengths last.
 __host__ __device__ constexpr int p2_radix(int N, int V, int i) {
   int NS = 1, R = 1;
   for (int p = 0; p <= i; ++p) {
@@ -460,19 +481,20 @@ __host__ __device__ constexpr int p2_span(int N, int V, bool inv, int i) {
   return NS;
 }
 
-// Pass I of a transform over the values x[j] = X[t + j*N/V] held by thread t (V
-// per thread, so a pass of radix R is V/R butterflies per thread).  Writes the
-// results to Y, or (TOREG, the forward's last pass) back into x: that pass's
-// butterfly m reads and writes the positions t + (m + M*r)*T, which are x's own.
-template <int N, int V, bool INV, int I, bool TOREG>
+// Pass I of the forward transform over the values x[j] = X[t + j*N/V] held by
+// thread t (V per thread, so a pass of radix R is V/R butterflies per thread):
+// twiddles, radix-R DFT, results written to Y at base + r*NS -- or, for the last
+// pass (TOREG), back into x: that pass's butterfly m reads and writes the
+// positions t + (m + M*r)*T, which are x's own.
+template <int N, int V, int I, bool TOREG>
 __device__ __forceinline__ void p2_pass(float2 (&x)[V], int t, const float2 *__restrict__ tw, float2 *Y) {
   constexpr int T = N / V;
-  constexpr int P = p2_npass(N, V);
-  constexpr int R = p2_radix(N, V, INV ? P - 1 - I : I);
-  constexpr int NS = p2_span(N, V, INV, I);
+  constexpr int R = p2_radix(N, V, I);
+  constexpr int NS = p2_span(N, V, false, I);
   constexpr int M = V / R;  // butterflies per thread
   static_assert(V % R == 0, "values per thread must be a multiple of the radix");
-  static_assert(!TOREG || NS * R == N, "only a transform's last pass keeps its results in registers");
+  static_assert(!TOREG || NS * R == N, "only the last pass keeps its results in registers");
+  static_assert(TOREG || ((NS & (NS - 1)) == 0 && R != 3), "folded offsets need power-of-two spans and radices");
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     const int b = t + m * T;
@@ -482,26 +504,16 @@ __device__ __forceinline__ void p2_pass(float2 (&x)[V], int t, const float2 *__r
     for (int r = 0; r < R; ++r) v[r] = x[m + M * r];  // X[b + r*N/R]
     if constexpr (NS > 1) {
 #pragma unroll
-      for (int r = 1; r < R; ++r) {
-        float2 w = __ldg(&tw[r * k * (N / (NS * R))]);
-        if (INV) w.y = -w.y;
-        v[r] = cmul(v[r], w);
-      }
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(&tw[r * k * (N / (NS * R))]));
     }
-    dft_r<R, INV>(v);
+    dft_r<R, false>(v);
     if constexpr (TOREG) {
 #pragma unroll
       for (int r = 0; r < R; ++r) x[m + M * r] = v[r];
     } else {
-      const int base = (b - k) * R + k;
-      if constexpr ((NS & (NS - 1)) == 0 && R != 3) {  // power-of-two span and radix: offsets fold (swz_add)
-        const int sb = swz(base);
+      const int sb = swz((b - k) * R + k);
 #pragma unroll
-        for (int r = 0; r < R; ++r) Y[swz_add(sb, r * NS)] = v[r];
-      } else {  // the inverse of 3*2^k lengths: radix 3 first, then spans 3*2^j
-#pragma unroll
-        for (int r = 0; r < R; ++r) Y[swz(base + r * NS)] = v[r];
-      }
+      for (int r = 0; r < R; ++r) Y[swz_add(sb, r * NS)] = v[r];
     }
   }
 }
@@ -514,9 +526,9 @@ __device__ __forceinline__ void p2_forward(float2 (&x)[V], int t, const float2 *
                                            float2 *B) {
   constexpr int T = N / V;
   if constexpr (I == p2_npass(N, V) - 1) {
-    p2_pass<N, V, false, I, true>(x, t, tw, nullptr);
+    p2_pass<N, V, I, true>(x, t, tw, nullptr);
   } else {
-    p2_pass<N, V, false, I, false>(x, t, tw, A);
+    p2_pass<N, V, I, false>(x, t, tw, A);
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < V; ++j) x[j] = A[swz_add(swz(t), j * T)];
@@ -524,21 +536,63 @@ __device__ __forceinline__ void p2_forward(float2 (&x)[V], int t, const float2 *
   }
 }
 
-// Inverse transform from pass I on (x holds pass I's inputs, pass I writes A);
-// returns the buffer holding the natural-order result (after a barrier).
+// Pass I of the inverse transform: the transpose of forward pass PF = P-1-I
+// (the forward matrix is symmetric, so the conjugate of the reversed product of
+// its transposed passes is the unnormalised inverse).  It reads where pass PF
+// wrote (base + r*NS; for I = 0 the forward's last pass, whose values are still
+// in x), applies the inverse radix-R DFT and then the conjugate twiddles, and
+// leaves in x[m + M*r] the positions t + (m + M*r)*T that pass PF read.  So
+// every shared-memory access is one the forward already makes: lane-contiguous
+// stores, and loads in the forward's store pattern (bank-conflict-free in the
+// padded layout).
+template <int N, int V, int I>
+__device__ __forceinline__ void p2_ipass(float2 (&x)[V], int t, const float2 *__restrict__ tw, const float2 *Y) {
+  constexpr int T = N / V;
+  constexpr int PF = p2_npass(N, V) - 1 - I;
+  constexpr int R = p2_radix(N, V, PF);
+  constexpr int NS = p2_span(N, V, false, PF);
+  constexpr int M = V / R;
+  static_assert(I == 0 || ((NS & (NS - 1)) == 0 && R != 3), "folded offsets need power-of-two spans and radices");
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int b = t + m * T;
+    const int k = b % NS;
+    float2 v[R];
+    if constexpr (I == 0) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = x[m + M * r];
+    } else {
+      const int sb = swz((b - k) * R + k);
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = Y[swz_add(sb, r * NS)];
+    }
+    dft_r<R, true>(v);
+    if constexpr (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = __ldg(&tw[r * k * (N / (NS * R))]);
+        w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[m + M * r] = v[r];
+  }
+}
+
+// Inverse transform from pass I on (I = 0: x holds the weighted spectrum as the
+// forward left it).  Pass I reads B (I > 0) and stores its results, in natural
+// positions, to A; returns the buffer holding the result (after a barrier).
 template <int N, int V, int I>
 __device__ __forceinline__ float2 *p2_inverse(float2 (&x)[V], int t, const float2 *__restrict__ tw, float2 *A,
                                               float2 *B) {
   constexpr int T = N / V;
-  p2_pass<N, V, true, I, false>(x, t, tw, A);
-  __syncthreads();
-  if constexpr (I == p2_npass(N, V) - 1) {
-    return A;
-  } else {
+  p2_ipass<N, V, I>(x, t, tw, B);
 #pragma unroll
-    for (int j = 0; j < V; ++j) x[j] = A[swz_add(swz(t), j * T)];
-    return p2_inverse<N, V, I + 1>(x, t, tw, B, A);
-  }
+  for (int j = 0; j < V; ++j) A[swz_add(swz(t), j * T)] = x[j];
+  __syncthreads();
+  if constexpr (I == p2_npass(N, V) - 1) return A;
+  else return p2_inverse<N, V, I + 1>(x, t, tw, B, A);
 }
 
 template <int N, int V, int FMT, int STORE>
@@ -607,10 +661,10 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
     if (sx0 >= 0 && sx0 < N) return sc(sx0);
     return make_float2(0.0f, 0.0f);
   };
-  // pack into the staging format with the reference's fill rule (main.rs:386-406):
-  // each thread takes two consecutive elements e, e+1 (PW is even), whose pairs
-  // need the final values at k, k+1, k+2 (k = e - padL), computed straight from
-  // the inverse (no second exchange)
+  // pack into the staging format with the reference's fill rule (main.rs:386-406).
+  // A warp takes 31 consecutive elements e at a time: lane l computes the final
+  // value at k = e - padL straight from the inverse (no second exchange) and
+  // takes the value at k + 1 from lane l + 1; lane 31 only supplies its value.
   const float fillv = a.fill ? a.fill[v] : 0.0f;
   auto fill = [&](int k) -> float2 {
     if (a.fill_mode == TG_FILL_ZERO) return make_float2(0.0f, 0.0f);
@@ -619,53 +673,43 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
   };
   float hmax = 0.0f;  // largest |value| packed into FP16 by this thread
   const size_t row0 = (size_t)v * a.rows_alloc;
-  for (int e = 2 * t; e < a.PW; e += 2 * T) {
+  const int lane = t & 31;
+  static_assert(T % 32 == 0, "whole warps per row pair");
+  for (int e0 = (t >> 5) * 31; e0 < a.PW; e0 += (T / 32) * 31) {  // warp-uniform bounds
+    const int e = e0 + lane;
     const int k = e - a.padL;
-    float2 f0 = make_float2(0.0f, 0.0f), f1 = f0, f2 = f0;
-    if (k >= 0 && k < N) f0 = fin(k);
-    if (k + 1 >= 0 && k + 1 < N) f1 = fin(k + 1);
-    if (k + 2 >= 0 && k + 2 < N) f2 = fin(k + 2);
-    float2 lo0 = f0, hi0 = f1, lo1 = f1, hi1 = f2;  // (row[k], row[k+1]) and (row[k+1], row[k+2])
-    if (!(k >= 0 && k + 1 < N)) lo0 = hi0 = fill(k);
-    if (!(k + 1 >= 0 && k + 2 < N)) lo1 = hi1 = fill(k + 1);
-    if (!has1) lo0.y = hi0.y = lo1.y = hi1.y = 0.0f;
+    float2 lo = make_float2(0.0f, 0.0f);
+    if (k >= 0 && k < N) lo = fin(k);
+    float2 hi = make_float2(__shfl_down_sync(0xffffffffu, lo.x, 1), __shfl_down_sync(0xffffffffu, lo.y, 1));
+    if (lane == 31 || e >= a.PW) continue;
+    if (!(k >= 0 && k + 1 < N)) lo = hi = fill(k);
+    if (!has1) lo.y = hi.y = 0.0f;
     if (FMT == FMT_ROWPAIR) {
       uint8_t *out = reinterpret_cast<uint8_t *>(a.out) +
                      (row0 + jp) * (size_t)a.PW * (STORE == TG_STORE_FP32 ? 16 : 8);
       if (STORE == TG_STORE_FP32) {
-        float4 *o = reinterpret_cast<float4 *>(out) + e;
-        o[0] = make_float4(lo0.x, lo0.y, hi0.x, hi0.y);
-        o[1] = make_float4(lo1.x, lo1.y, hi1.x, hi1.y);
+        reinterpret_cast<float4 *>(out)[e] = make_float4(lo.x, lo.y, hi.x, hi.y);
       } else {
         using PK = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>;
-        const float d0x = __fsub_rn(hi0.x, lo0.x), d0y = __fsub_rn(hi0.y, lo0.y);
-        const float d1x = __fsub_rn(hi1.x, lo1.x), d1y = __fsub_rn(hi1.y, lo1.y);
-        range_track<STORE>(hmax, lo0.x, lo0.y);
-        range_track<STORE>(hmax, lo1.x, lo1.y);
-        range_track<STORE>(hmax, d0x, d0y);
-        range_track<STORE>(hmax, d1x, d1y);
-        reinterpret_cast<uint4 *>(out)[e >> 1] =
-            make_uint4(PK::h2(lo0.x, lo0.y), PK::h2(d0x, d0y), PK::h2(lo1.x, lo1.y), PK::h2(d1x, d1y));
+        const float d0 = __fsub_rn(hi.x, lo.x), d1 = __fsub_rn(hi.y, lo.y);
+        range_track<STORE>(hmax, lo.x, lo.y);
+        range_track<STORE>(hmax, d0, d1);
+        reinterpret_cast<uint2 *>(out)[e] = make_uint2(PK::h2(lo.x, lo.y), PK::h2(d0, d1));
       }
     } else {
       const int eb = STORE == TG_STORE_FP32 ? 8 : 4;
       uint8_t *o0 = reinterpret_cast<uint8_t *>(a.out) + (row0 + r0) * (size_t)a.PW * eb;
       uint8_t *o1 = o0 + (size_t)a.PW * eb;
       if (STORE == TG_STORE_FP32) {
-        reinterpret_cast<float4 *>(o0)[e >> 1] = make_float4(lo0.x, hi0.x, lo1.x, hi1.x);
-        if (has1) reinterpret_cast<float4 *>(o1)[e >> 1] = make_float4(lo0.y, hi0.y, lo1.y, hi1.y);
+        reinterpret_cast<float2 *>(o0)[e] = make_float2(lo.x, hi.x);
+        if (has1) reinterpret_cast<float2 *>(o1)[e] = make_float2(lo.y, hi.y);
       } else {
         using PK = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>;
-        const float d0x = __fsub_rn(hi0.x, lo0.x), d0y = __fsub_rn(hi0.y, lo0.y);
-        const float d1x = __fsub_rn(hi1.x, lo1.x), d1y = __fsub_rn(hi1.y, lo1.y);
-        range_track<STORE>(hmax, lo0.x, lo1.x);
-        range_track<STORE>(hmax, d0x, d1x);
-        if (has1) {
-          range_track<STORE>(hmax, lo0.y, lo1.y);
-          range_track<STORE>(hmax, d0y, d1y);
-        }
-        reinterpret_cast<uint2 *>(o0)[e >> 1] = make_uint2(PK::h2(lo0.x, d0x), PK::h2(lo1.x, d1x));
-        if (has1) reinterpret_cast<uint2 *>(o1)[e >> 1] = make_uint2(PK::h2(lo0.y, d0y), PK::h2(lo1.y, d1y));
+        const float d0 = __fsub_rn(hi.x, lo.x), d1 = __fsub_rn(hi.y, lo.y);
+        range_track<STORE>(hmax, lo.x, d0);
+        if (has1) range_track<STORE>(hmax, lo.y, d1);
+        reinterpret_cast<uint32_t *>(o0)[e] = PK::h2(lo.x, d0);
+        if (has1) reinterpret_cast<uint32_t *>(o1)[e] = PK::h2(lo.y, d1);
       }
     }
   }
