@@ -19,6 +19,7 @@
 
 #include "tg_internal.h"
 #include "fft.cuh"
+#include "f32x2.cuh"
 
 namespace tg {
 
@@ -409,26 +410,46 @@ __global__ void __launch_bounds__(256) filter_kernel(FilterArgs a) {
 // transform's first pass loads, and the epilogue works on the complex pairs
 // (row 2j in .x, row 2j+1 in .y) without splitting them.
 // ---------------------------------------------------------------------------
+// Radix-4 butterfly with the plain complex sums and differences on the packed
+// f32x2 pipe (one instruction per complex add); the ones that meet a rotation by
+// -+i stay scalar, where the swap and sign fold into the adds.  ROT2: v[2]
+// arrives still to be rotated by -+i (the radix-8 butterfly's third odd term).
+template <bool INV, bool ROT2> __device__ __forceinline__ void bfly4_p(float2 *v) {
+  float2 a0, a1;
+  if constexpr (ROT2) {
+    const float2 r = rot<INV>(v[2]);
+    a0 = cadd(v[0], r);
+    a1 = csub(v[0], r);
+  } else {
+    a0 = cadd_p(v[0], v[2]);
+    a1 = csub_p(v[0], v[2]);
+  }
+  const float2 b0 = cadd_p(v[1], v[3]), b1 = rot<INV>(csub_p(v[1], v[3]));
+  v[0] = cadd_p(a0, b0);
+  v[1] = cadd(a1, b1);
+  v[2] = csub_p(a0, b0);
+  v[3] = csub(a1, b1);
+}
+
 template <bool INV> __device__ __forceinline__ void dft8(float2 *v) {
   const float h = 0.707106781186547524400844362104849039f;  // 1/sqrt(2)
   float2 t[4], u[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    t[j] = cadd(v[j], v[j + 4]);
-    u[j] = csub(v[j], v[j + 4]);
+    t[j] = cadd_p(v[j], v[j + 4]);
+    u[j] = csub_p(v[j], v[j + 4]);
   }
-  // u_j *= exp(-+2 pi i j / 8)
+  // u_j *= exp(-+2 pi i j / 8) (u_2's factor -+i is folded into its butterfly)
   {
     const float2 d = u[1];
     u[1] = INV ? make_float2(h * (d.x - d.y), h * (d.x + d.y)) : make_float2(h * (d.x + d.y), h * (d.y - d.x));
   }
-  u[2] = rot<INV>(u[2]);
   {
     const float2 d = u[3];
     u[3] = INV ? make_float2(-h * (d.x + d.y), h * (d.x - d.y)) : make_float2(h * (d.y - d.x), -h * (d.x + d.y));
   }
-  bfly<4, INV>(t, nullptr, 4);
-  bfly<4, INV>(u, nullptr, 4);
+  bfly4_p<INV, false>(t);
+  bfly4_p<INV, true>(u);
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
     v[2 * m] = t[m];
@@ -438,7 +459,12 @@ template <bool INV> __device__ __forceinline__ void dft8(float2 *v) {
 
 template <int R, bool INV> __device__ __forceinline__ void dft_r(float2 *v) {
   if constexpr (R == 8) dft8<INV>(v);
-  else bfly<R, INV>(v, nullptr, R);
+  else if constexpr (R == 4) bfly4_p<INV, false>(v);
+  else if constexpr (R == 2) {
+    const float2 a = v[0], b = v[1];
+    v[0] = cadd_p(a, b);
+    v[1] = csub_p(a, b);
+  } else bfly<R, INV>(v, nullptr, R);
 }
 
 // Shared-memory position of row element e: one padding slot after every 16
@@ -716,8 +742,9 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
   range_report<STORE>(a, hmax);
 }
 
+// at least 4 CTAs of 256 threads per SM (64 registers): the kernel is latency-bound
 template <int N, int V, int FMT, int STORE>
-__global__ void __launch_bounds__(N / V) filter_p2_kernel(FilterArgs a) {
+__global__ void __launch_bounds__(N / V, N / V == 256 ? 4 : 1) filter_p2_kernel(FilterArgs a) {
   filter_p2_body<N, V, FMT, STORE>(a, blockIdx.x, blockIdx.y);
 }
 
@@ -725,7 +752,7 @@ __global__ void __launch_bounds__(N / V) filter_p2_kernel(FilterArgs a) {
 // belongs to series j with blk0[j] <= b < blk0[j+1] ((ny+1)/2 row pairs x views
 // each); every series' rows come out as in its own launch.
 template <int N, int V, int FMT, int STORE>
-__global__ void __launch_bounds__(N / V) filter_p2_batch_kernel(FilterBatchDev fb) {
+__global__ void __launch_bounds__(N / V, N / V == 256 ? 4 : 1) filter_p2_batch_kernel(FilterBatchDev fb) {
   __shared__ __align__(16) FilterArgs s_a;
   __shared__ int s_j;
   if (threadIdx.x == 0) {

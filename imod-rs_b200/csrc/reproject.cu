@@ -147,6 +147,13 @@ __device__ __forceinline__ void fp_fast_body(const FpArgs &a, const int bx, cons
   float acc[S];
 #pragma unroll
   for (int s = 0; s < S; ++s) acc[s] = 0.0f;
+  // blended copy (one x-tilt for all views): its rows are blends, so this path is
+  // within a tolerance of the reference, not bit-exact, and the products are fused
+  // into packed accumulator pairs (one fma.f32x2 per two rows of a column visit)
+  constexpr bool FUSED = XT && IL;
+  uint64_t acc2[FUSED ? S / 2 : 1];
+#pragma unroll
+  for (int s = 0; s < (FUSED ? S / 2 : 1); ++s) acc2[s] = 0;
   // ((dx*cos)*cos_xt + t2) + cx, exactly as main.rs:842; fo is the column as a float
   // (carried along with the integer column: integers are exact in f32)
   auto X = [&](float fo, float t2) {
@@ -188,11 +195,16 @@ __device__ __forceinline__ void fp_fast_body(const FpArgs &a, const int bx, cons
 #pragma unroll
         for (int k = 0; k < S / 4; ++k) {
           const float4 q4 = __ldg(q + (size_t)k * a.onx);
-          const float2 pa = up2(mul2(pk2(q4.x, q4.y), w2)), pb = up2(mul2(pk2(q4.z, q4.w), w2));
-          acc[4 * k + 0] = __fadd_rn(acc[4 * k + 0], pa.x);
-          acc[4 * k + 1] = __fadd_rn(acc[4 * k + 1], pa.y);
-          acc[4 * k + 2] = __fadd_rn(acc[4 * k + 2], pb.x);
-          acc[4 * k + 3] = __fadd_rn(acc[4 * k + 3], pb.y);
+          if constexpr (FUSED) {
+            acc2[2 * k] = fma2(pk2(q4.x, q4.y), w2, acc2[2 * k]);
+            acc2[2 * k + 1] = fma2(pk2(q4.z, q4.w), w2, acc2[2 * k + 1]);
+          } else {
+            const float2 pa = up2(mul2(pk2(q4.x, q4.y), w2)), pb = up2(mul2(pk2(q4.z, q4.w), w2));
+            acc[4 * k + 0] = __fadd_rn(acc[4 * k + 0], pa.x);
+            acc[4 * k + 1] = __fadd_rn(acc[4 * k + 1], pa.y);
+            acc[4 * k + 2] = __fadd_rn(acc[4 * k + 2], pb.x);
+            acc[4 * k + 3] = __fadd_rn(acc[4 * k + 3], pb.y);
+          }
         }
       } else if (!XT) {
         const float *vrow = vz + (size_t)r0 * sstride + ox;
@@ -248,6 +260,14 @@ __device__ __forceinline__ void fp_fast_body(const FpArgs &a, const int bx, cons
           }
         }
       }
+    }
+  }
+  if constexpr (FUSED) {
+#pragma unroll
+    for (int k = 0; k < S / 2; ++k) {
+      const float2 u = up2(acc2[k]);
+      acc[2 * k] = u.x;
+      acc[2 * k + 1] = u.y;
     }
   }
 #pragma unroll
