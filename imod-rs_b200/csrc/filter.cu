@@ -506,6 +506,82 @@ __host__ __device__ constexpr int p2_span(int N, int V, bool inv, int i) {
   for (int p = 0; p < i; ++p) NS *= p2_radix(N, V, inv ? p2_npass(N, V) - 1 - p : p);
   return NS;
 }
+// offset of forward pass i's twiddles in the per-pass table: (R-1)*NS entries
+// per earlier pass with twiddles (NS > 1; n - R0 entries in all, R0 the first radix)
+__host__ __device__ constexpr int p2_twoff(int N, int V, int i) {
+  int off = 0;
+  for (int p = 1; p < i; ++p) off += (p2_radix(N, V, p) - 1) * p2_span(N, V, false, p);
+  return off;
+}
+// Shared-memory layout of the buffer a pass writes.  LAY_PAD (swz): one slot of
+// padding per 16 values; LAY_XOR8: no padding, bit 3 of the slot flipped in odd
+// 64-value blocks -- for the output of a radix-8 pass at span 8, whose strided
+// stores put two groups of 8 lanes 64 values apart, 4 slots apart (two-way bank
+// conflicts) in the padded layout and 8 apart here; LAY_LIN: plain, for the
+// inverse's result, which the staging epilogue reads at consecutive positions.
+// Each layout keeps 16 consecutive values of an aligned block in 16 distinct
+// bank pairs, so the lane-contiguous accesses stay conflict-free.
+enum { LAY_PAD = 0, LAY_XOR8 = 1, LAY_LIN = 2 };
+__host__ __device__ constexpr int p2_layout(int N, int V, int p) {
+  return (p2_radix(N, V, p) == 8 && p2_span(N, V, false, p) == 8) ? LAY_XOR8 : LAY_PAD;
+}
+// slot of element t + j*T (lane-contiguous accesses)
+template <int LAY, int T> __device__ __forceinline__ int p2_cslot(int t, int j) {
+  if constexpr (LAY == LAY_PAD) {
+    return swz_add(swz(t), j * T);
+  } else if constexpr (LAY == LAY_LIN) {
+    return t + j * T;
+  } else if constexpr (T % 128 == 0) {
+    return (t ^ (((t >> 6) & 1) << 3)) + j * T;  // bit 6 of t + j*T is bit 6 of t
+  } else {
+    const int e = t + j * T;
+    return e ^ (((e >> 6) & 1) << 3);
+  }
+}
+// slots of base + r*NS, r = 0..R-1 (a pass's strided accesses), as a base per
+// parity of r plus compile-time offsets: even r at sb[0] + r*NS, odd at sb[1] + r*NS
+// (LAY_PAD: offsets folded as in swz_add; LAY_XOR8, radix 8 at span 8: base + 8r
+// stays in base's 64-value block, so the flip is a +-8 on the parity of r)
+template <int LAY, int R, int NS> __device__ __forceinline__ void p2_sslot(int base, int (&sb)[2]) {
+  if constexpr (LAY == LAY_PAD) {
+    sb[0] = sb[1] = swz(base);
+  } else {
+    static_assert(R == 8 && NS == 8, "the flipped layout serves the radix-8 pass at span 8");
+    const int q8 = ((base >> 6) & 1) << 3;
+    sb[0] = base + q8;
+    sb[1] = base - q8;
+  }
+}
+template <int LAY> __device__ __forceinline__ int p2_soff(int off) {
+  return LAY == LAY_PAD ? off + (off >> 4) : off;
+}
+
+// values per thread of the register-resident kernel for rows of n samples (0: none)
+static int p2_values(int n) {
+  switch (n) {
+    case 256: case 512: case 1024: case 2048: case 4096: return 8;
+    case 384: return 12;
+    case 768: case 1536: case 3072: return 24;
+    default: return 0;
+  }
+}
+
+bool p2_twiddle_table(int n, std::vector<float2> &out) {
+  out.clear();
+  const int V = p2_values(n);
+  if (!V) return false;
+  out.resize((size_t)n - p2_radix(n, V, 0));
+  for (int p = 0; p < p2_npass(n, V); ++p) {
+    const int R = p2_radix(n, V, p), NS = p2_span(n, V, false, p), off = p2_twoff(n, V, p);
+    if (NS == 1) continue;
+    for (int r = 1; r < R; ++r)
+      for (int k = 0; k < NS; ++k) {
+        const double a = -2.0 * M_PI * (double)(r * k) / (double)(NS * R);
+        out[(size_t)off + (size_t)(r - 1) * NS + k] = make_float2((float)cos(a), (float)sin(a));
+      }
+  }
+  return true;
+}
 
 // Pass I of the forward transform over the values x[j] = X[t + j*N/V] held by
 // thread t (V per thread, so a pass of radix R is V/R butterflies per thread):
@@ -529,17 +605,20 @@ __device__ __forceinline__ void p2_pass(float2 (&x)[V], int t, const float2 *__r
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = x[m + M * r];  // X[b + r*N/R]
     if constexpr (NS > 1) {
+      const float2 *tp = tw + p2_twoff(N, V, I) + k;
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(&tw[r * k * (N / (NS * R))]));
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(tp + (r - 1) * NS));
     }
     dft_r<R, false>(v);
     if constexpr (TOREG) {
 #pragma unroll
       for (int r = 0; r < R; ++r) x[m + M * r] = v[r];
     } else {
-      const int sb = swz((b - k) * R + k);
+      constexpr int LAY = p2_layout(N, V, I);
+      int sb[2];
+      p2_sslot<LAY, R, NS>((b - k) * R + k, sb);
 #pragma unroll
-      for (int r = 0; r < R; ++r) Y[swz_add(sb, r * NS)] = v[r];
+      for (int r = 0; r < R; ++r) Y[sb[r & 1] + p2_soff<LAY>(r * NS)] = v[r];
     }
   }
 }
@@ -557,7 +636,7 @@ __device__ __forceinline__ void p2_forward(float2 (&x)[V], int t, const float2 *
     p2_pass<N, V, I, false>(x, t, tw, A);
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < V; ++j) x[j] = A[swz_add(swz(t), j * T)];
+    for (int j = 0; j < V; ++j) x[j] = A[p2_cslot<p2_layout(N, V, I), T>(t, j)];
     p2_forward<N, V, I + 1>(x, t, tw, B, A);
   }
 }
@@ -588,15 +667,18 @@ __device__ __forceinline__ void p2_ipass(float2 (&x)[V], int t, const float2 *__
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = x[m + M * r];
     } else {
-      const int sb = swz((b - k) * R + k);
+      constexpr int LAY = p2_layout(N, V, PF);
+      int sb[2];
+      p2_sslot<LAY, R, NS>((b - k) * R + k, sb);
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[r] = Y[swz_add(sb, r * NS)];
+      for (int r = 0; r < R; ++r) v[r] = Y[sb[r & 1] + p2_soff<LAY>(r * NS)];
     }
     dft_r<R, true>(v);
     if constexpr (NS > 1) {
+      const float2 *tp = tw + p2_twoff(N, V, PF) + k;
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        float2 w = __ldg(&tw[r * k * (N / (NS * R))]);
+        float2 w = __ldg(tp + (r - 1) * NS);
         w.y = -w.y;
         v[r] = cmul(v[r], w);
       }
@@ -614,8 +696,12 @@ __device__ __forceinline__ float2 *p2_inverse(float2 (&x)[V], int t, const float
                                               float2 *B) {
   constexpr int T = N / V;
   p2_ipass<N, V, I>(x, t, tw, B);
+  // the next pass reads in the strided pattern of forward pass P-2-I: that pass's
+  // layout; the last pass's result is plain
+  constexpr int P = p2_npass(N, V);
+  constexpr int LAY = I == P - 1 ? LAY_LIN : p2_layout(N, V, P - 2 - I);
 #pragma unroll
-  for (int j = 0; j < V; ++j) A[swz_add(swz(t), j * T)] = x[j];
+  for (int j = 0; j < V; ++j) A[p2_cslot<LAY, T>(t, j)] = x[j];
   __syncthreads();
   if constexpr (I == p2_npass(N, V) - 1) return A;
   else return p2_inverse<N, V, I + 1>(x, t, tw, B, A);
@@ -643,7 +729,7 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
     }
     x[j] = make_float2(x0, x1);
   }
-  p2_forward<N, V, 0>(x, t, a.tw, A, B);
+  p2_forward<N, V, 0>(x, t, a.tw2, A, B);
   // x[j] = spectrum value t + j*T: x the radial weight, and for 2^k lengths the
   // 1/n of the inverse too (a power of two: exact, and exact through the
   // inverse's linear arithmetic, so the result is the one of scaling afterwards)
@@ -657,10 +743,10 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
   // the forward's last exchange read buffer A (odd pass count) or B; the
   // inverse's first pass writes the other one
   constexpr int P = p2_npass(N, V);
-  const float2 *Rr = P % 2 == 0 ? p2_inverse<N, V, 0>(x, t, a.tw, B, A) : p2_inverse<N, V, 0>(x, t, a.tw, A, B);
+  const float2 *Rr = P % 2 == 0 ? p2_inverse<N, V, 0>(x, t, a.tw2, B, A) : p2_inverse<N, V, 0>(x, t, a.tw2, A, B);
   const float inv_n = a.inv_n;
   auto sc = [&](int k) {
-    const float2 z = Rr[swz(k)];
+    const float2 z = Rr[k];  // plain layout
     return POW2 ? z : make_float2(__fmul_rn(z.x, inv_n), __fmul_rn(z.y, inv_n));
   };
   // final value of both rows at column k (0 <= k < N): the cosine stretch
@@ -782,7 +868,7 @@ template <int N, int V, int FMT, int STORE> static void launch_p2(const FilterAr
 }
 
 template <int FMT, int STORE> static bool try_p2(const FilterArgs &a, cudaStream_t st) {
-  if (!a.weights || a.conv_h || getenv("TG_FILTER_GENERIC")) return false;
+  if (!a.weights || a.conv_h || !a.tw2 || getenv("TG_FILTER_GENERIC")) return false;
   switch (a.nx) {
     case 256: launch_p2<256, 8, FMT, STORE>(a, st); return true;
     case 512: launch_p2<512, 8, FMT, STORE>(a, st); return true;
@@ -806,7 +892,7 @@ template <int FMT, int STORE> static void launch_f(const FilterArgs &a, cudaStre
 }
 
 int filter_batch_width(const FilterArgs &a) {
-  if (!a.weights || a.conv_h || getenv("TG_FILTER_GENERIC")) return 0;
+  if (!a.weights || a.conv_h || !a.tw2 || getenv("TG_FILTER_GENERIC")) return 0;
   switch (a.nx) {
     case 256: case 512: case 1024: case 2048: case 4096: case 384: case 768: case 1536: case 3072: return a.nx;
     default: return 0;

@@ -295,6 +295,7 @@ FilterArgs filter_args(tg_session *s, bool residual) {
   f.out = s->d_pairs;
   f.weights = s->o.no_weight ? nullptr : s->d_weights;
   f.tw = s->d_tw;
+  f.tw2 = s->has_tw2 ? s->d_tw + s->nx : nullptr;
   f.conv_h = s->use_conv ? s->d_conv : nullptr;
   f.stretch = residual ? nullptr : s->d_stretch;
   f.fill = s->d_means;
@@ -669,7 +670,7 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
       (rc = dalloc(s, &s->d_part, (size_t)s->ny * ntiles * sizeof(StatPartial))) ||
       (rc = dalloc(s, &s->d_slice_stats, (size_t)s->ny * 12)) || (rc = dalloc(s, &s->d_stats3, 16)) ||
       (rc = dalloc(s, &s->d_vg, (size_t)s->nviews * 16)) || (rc = dalloc(s, &s->d_vg2, (size_t)s->nviews * 16)) ||
-      (rc = dalloc(s, &s->d_weights, (size_t)s->nx * 4)) || (rc = dalloc(s, &s->d_tw, (size_t)s->nx * 8)) ||
+      (rc = dalloc(s, &s->d_weights, (size_t)s->nx * 4)) || (rc = dalloc(s, &s->d_tw, (size_t)s->nx * 16)) ||
       (rc = dalloc(s, &s->d_stretch, (size_t)s->nviews * 4)) || (rc = dalloc(s, &s->d_err, 16)))
     return fail(rc);
   if (opt->log_transform && (rc = dalloc(s, &s->d_logd, nproj * 4))) return fail(rc);
@@ -720,11 +721,15 @@ int tg::session_create_ex(const tg_geometry *g, const tg_options *opt, cudaMemPo
 
   std::vector<float> wt(s->nx);
   weight_table(s->nx, opt->radial_cutoff, opt->radial_falloff, opt->exact_filter_size, opt->hamming, wt.data());
-  std::vector<float2> tw(s->nx);
+  // [0, nx): exp(-2 pi i k/nx); [nx, 2 nx - 1): the register-resident kernel's
+  // per-pass table, for the widths that have that kernel
+  std::vector<float2> tw(2 * (size_t)s->nx, make_float2(0.0f, 0.0f)), tw2;
   for (int k = 0; k < s->nx; ++k) {
     double a = -2.0 * M_PI * (double)k / (double)s->nx;
     tw[k] = make_float2((float)cos(a), (float)sin(a));
   }
+  s->has_tw2 = p2_twiddle_table(s->nx, tw2);
+  std::copy(tw2.begin(), tw2.end(), tw.begin() + s->nx);
   if (s->use_conv) {
     // h[m] = (1/n) * sum_k w[k] exp(2 pi i k m / n)  (w real and even)
     std::vector<float> h(s->nx);

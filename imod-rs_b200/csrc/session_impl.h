@@ -47,7 +47,8 @@ struct tg_session {  // one tilt series resident on a device
   float *d_slice_stats = nullptr, *d_stats3 = nullptr;
   float4 *d_vg = nullptr, *d_vg2 = nullptr;
   float *d_weights = nullptr, *d_conv = nullptr, *d_stretch = nullptr;
-  float2 *d_tw = nullptr;
+  float2 *d_tw = nullptr;  // 2 nx: plain twiddles, then the register-resident filter's per-pass table
+  bool has_tw2 = false;
   int *d_err = nullptr;
   int4 *d_lvinfo = nullptr;
   int *d_lgoff = nullptr;

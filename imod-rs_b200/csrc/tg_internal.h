@@ -1,5 +1,6 @@
 // tg_internal.h -- shared declarations of libtiltgpu (kernels + host plumbing).
 #pragma once
+#include <vector>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -57,6 +58,7 @@ struct FilterArgs {
   void *out;                // staged format
   const float *weights;     // n weights, nullptr = no R-weighting
   const float2 *tw;         // n twiddles exp(-2 pi i k/n)
+  const float2 *tw2;        // register-resident kernel's per-pass twiddles (p2_twiddle_table), or nullptr
   const float *conv_h;      // circulant kernel for n without a radix plan (else nullptr)
   const float *stretch;     // per view 1/cos (f32) or 0: no stretch; nullptr = none
   const float *fill;        // per view fill value for mean mode
@@ -69,6 +71,11 @@ struct FilterArgs {
   int *err;                 // session error word: bit 2 set when a value exceeds the FP16 range
 };
 void launch_filter(const FilterArgs &a, cudaStream_t st);
+// Twiddles of the register-resident filter kernel for rows of n samples, per
+// forward pass p with span NS > 1 and radix R: exp(-2 pi i r k / (NS R)) at
+// offset_p + (r-1)*NS + k (k-major, so a warp's lanes read neighbouring entries);
+// fewer than n entries in all.  False (table empty) when n has no such kernel.
+bool p2_twiddle_table(int n, std::vector<float2> &out);
 // ---- the register-resident filter over many series of one width in one launch ----
 struct FilterBatchDev {
   const FilterArgs *jobs;   // device array
