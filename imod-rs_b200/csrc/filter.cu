@@ -58,7 +58,9 @@ struct LogTable {
   float inv[257];
   double nl[257];
 };
-__device__ __forceinline__ float log_sample_fast(float x, const LogTable &lt) {
+// The evaluation without a branch: the rounded value and whether it is decided
+// (ok false: take log_sample), so that several samples' FP64 chains interleave.
+__device__ __forceinline__ float log_fast_core(float x, const LogTable &lt, bool &ok) {
   x = fmaxf(x, 0.001f);
   const int ix = __float_as_int(x);
   const int e = (ix - 0x3f400000) >> 23;
@@ -78,8 +80,13 @@ __device__ __forceinline__ float log_sample_fast(float x, const LogTable &lt) {
   float half_ulp = __int_as_float((ia & 0x7f800000) - (24 << 23));  // half the spacing above |f|
   if ((ia & 0x7fffff) == 0) half_ulp *= 0.5f;                        // below a power of two: half that
   const float dist = __double2float_rn(fabs(z - (double)f));
-  if (ix < 0x7f800000 && (ia & 0x7f800000) > (24 << 23) && dist + af * 0x1p-40f < half_ulp) return f;
-  return log_sample(x);
+  ok = ix < 0x7f800000 && (ia & 0x7f800000) > (24 << 23) && dist + af * 0x1p-40f < half_ulp;
+  return f;
+}
+__device__ __forceinline__ float log_sample_fast(float x, const LogTable &lt) {
+  bool ok;
+  const float f = log_fast_core(x, lt, ok);
+  return ok ? f : log_sample(x);
 }
 
 // the 257 centres' (inv_j, -ln inv_j) of log_sample_fast
@@ -92,10 +99,20 @@ __device__ __forceinline__ void log_table(LogTable &lt) {
   __syncthreads();
 }
 
+// four samples: the four evaluations first (independent FP64 chains), the rare
+// undecided ones after
 template <bool LOG> __device__ __forceinline__ float4 log4(float4 x, const LogTable &lt) {
-  return LOG ? make_float4(log_sample_fast(x.x, lt), log_sample_fast(x.y, lt), log_sample_fast(x.z, lt),
-                           log_sample_fast(x.w, lt))
-             : x;
+  if (!LOG) return x;
+  bool k0, k1, k2, k3;
+  float4 r = make_float4(log_fast_core(x.x, lt, k0), log_fast_core(x.y, lt, k1), log_fast_core(x.z, lt, k2),
+                         log_fast_core(x.w, lt, k3));
+  if (!(k0 && k1 && k2 && k3)) {
+    if (!k0) r.x = log_sample(x.x);
+    if (!k1) r.y = log_sample(x.y);
+    if (!k2) r.z = log_sample(x.z);
+    if (!k3) r.w = log_sample(x.w);
+  }
+  return r;
 }
 
 template <bool LOG>
