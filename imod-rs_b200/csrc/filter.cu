@@ -49,13 +49,13 @@ __device__ __forceinline__ float log_sample(float x) { return (float)log10((doub
 // within 2^-44 relative of log10 x (a CPU check of this evaluation over 2.5e7
 // samples against the FP64 log10 found at most 2^-47.6), so z rounded to float
 // is the correctly rounded log unless z lies within 2^-40 |z| of a midpoint
-// between floats; those samples (about 2 in 10^5), x = 1 (z = 0) and infinite
-// x take log_sample.  The table (shared memory) holds inv_j as float and
-// -ln inv_j as double, in separate arrays: neighbouring centres sit in
-// different banks, so the lanes of a warp (similar values, nearby centres)
-// rarely conflict.
+// between floats; those samples (about 2 in 10^5) and infinite x take
+// log_sample (x = 1 gives z = 0 exactly, the true value).  The table (shared memory) holds inv_j (a float value) and
+// -ln inv_j as doubles, in separate arrays.  The rounding test: z*(1 - 2^-40) and
+// z*(1 + 2^-40) round to the same float exactly when no midpoint between floats
+// lies between them, and the true value lies strictly inside that interval.
 struct LogTable {
-  float inv[257];
+  double inv[257];
   double nl[257];
 };
 // The evaluation without a branch: the rounded value and whether it is decided
@@ -66,7 +66,7 @@ __device__ __forceinline__ float log_fast_core(float x, const LogTable &lt, bool
   const int e = (ix - 0x3f400000) >> 23;
   const int mb = ix - (e << 23);
   const int j = (mb - 0x3f400000 + 0x4000) >> 15;
-  const double r = __fma_rn((double)__int_as_float(mb), (double)lt.inv[j], -1.0);
+  const double r = __fma_rn((double)__int_as_float(mb), lt.inv[j], -1.0);
   double p = __fma_rn(r, 0.2, -0.25);
   p = __fma_rn(r, p, 1.0 / 3.0);
   p = __fma_rn(r, p, -0.5);
@@ -74,14 +74,9 @@ __device__ __forceinline__ float log_fast_core(float x, const LogTable &lt, bool
   const double z = __dmul_rn(__dadd_rn(__fma_rn((double)e, 0.693147180559945309417232121458176568, lt.nl[j]),
                                        __dmul_rn(r, p)),
                              0.434294481903251827651128918916605082);  // ln 2, log10 e
-  const float f = __double2float_rn(z);
-  const float af = fabsf(f);
-  const int ia = __float_as_int(af);
-  float half_ulp = __int_as_float((ia & 0x7f800000) - (24 << 23));  // half the spacing above |f|
-  if ((ia & 0x7fffff) == 0) half_ulp *= 0.5f;                        // below a power of two: half that
-  const float dist = __double2float_rn(fabs(z - (double)f));
-  ok = ix < 0x7f800000 && (ia & 0x7f800000) > (24 << 23) && dist + af * 0x1p-40f < half_ulp;
-  return f;
+  const float lo = __double2float_rn(__dmul_rn(z, 1.0 - 0x1p-40)), hi = __double2float_rn(__dmul_rn(z, 1.0 + 0x1p-40));
+  ok = lo == hi && ix < 0x7f800000;
+  return lo;
 }
 __device__ __forceinline__ float log_sample_fast(float x, const LogTable &lt) {
   bool ok;
@@ -93,7 +88,7 @@ __device__ __forceinline__ float log_sample_fast(float x, const LogTable &lt) {
 __device__ __forceinline__ void log_table(LogTable &lt) {
   for (int i = threadIdx.x; i < 257; i += blockDim.x) {
     const float inv = __frcp_rn(__int_as_float(0x3f400000 + (i << 15)));
-    lt.inv[i] = inv;
+    lt.inv[i] = (double)inv;
     lt.nl[i] = -log((double)inv);
   }
   __syncthreads();
