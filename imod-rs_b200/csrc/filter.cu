@@ -759,7 +759,7 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
   const float inv_n = a.inv_n;
   auto sc = [&](int k) {
     const float2 z = Rr[k];  // plain layout
-    return POW2 ? z : make_float2(__fmul_rn(z.x, inv_n), __fmul_rn(z.y, inv_n));
+    return POW2 ? z : up2(mul2(pk2(z.x, z.y), pk2(inv_n, inv_n)));
   };
   // final value of both rows at column k (0 <= k < N): the cosine stretch
   // (main.rs:446-488) of the scaled inverse, or the scaled inverse itself
@@ -779,8 +779,9 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
     if (sx0 >= 0 && sx0 + 1 < N) {
       const float2 p0 = sc(sx0), p1 = sc(sx0 + 1);
       const float omf = __fsub_rn(1.0f, frac);
-      return make_float2(__fadd_rn(__fmul_rn(p0.x, omf), __fmul_rn(p1.x, frac)),
-                         __fadd_rn(__fmul_rn(p0.y, omf), __fmul_rn(p1.y, frac)));
+      // RN(RN(p0*(1-f)) + RN(p1*f)) for both rows on the packed pipe (each lane is
+      // the scalar operation: no product contracted into the sum)
+      return up2(add2(mul2(pk2(p0.x, p0.y), pk2(omf, omf)), mul2(pk2(p1.x, p1.y), pk2(frac, frac))));
     }
     if (sx0 >= 0 && sx0 < N) return sc(sx0);
     return make_float2(0.0f, 0.0f);
@@ -815,7 +816,8 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
         reinterpret_cast<float4 *>(out)[e] = make_float4(lo.x, lo.y, hi.x, hi.y);
       } else {
         using PK = Pack<STORE == TG_STORE_FP32 ? TG_STORE_FP16 : STORE>;
-        const float d0 = __fsub_rn(hi.x, lo.x), d1 = __fsub_rn(hi.y, lo.y);
+        const float2 d = csub_p(hi, lo);
+        const float d0 = d.x, d1 = d.y;
         range_track<STORE>(hmax, lo.x, lo.y);
         range_track<STORE>(hmax, d0, d1);
         reinterpret_cast<uint2 *>(out)[e] = make_uint2(PK::h2(lo.x, lo.y), PK::h2(d0, d1));
