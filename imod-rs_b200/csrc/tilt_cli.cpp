@@ -229,6 +229,8 @@ Args parse(int argc, char **argv) {
   if (!has_out) missing += "\n  --output <OUTPUT>";
   if (!has_tlt) missing += "\n  --tilt-file <TILT_FILE>";
   if (!missing.empty()) clap_error("the following required arguments were not provided:" + missing);
+  if ((!a.checkpoint.empty() || !a.resume.empty()) && (a.sirt <= 0 || a.gpu))
+    clap_error("--checkpoint and --resume need SIRT iterations (--sirt > 0, without --gpu)");
   return a;
 }
 

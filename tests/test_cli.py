@@ -98,3 +98,7 @@ def test_checkpoint_flags():
     assert r.returncode == 2 and "--checkpoint-every" in r.stderr
     r = run("-i", "a", "-o", "b", "-t", "c", "--resume")
     assert r.returncode == 2 and "a value is required for '--resume'" in r.stderr
+    r = run("-i", "a", "-o", "b", "-t", "c", "--resume", "s.mrc")
+    assert r.returncode == 2 and "need SIRT iterations" in r.stderr
+    r = run("-i", "a", "-o", "b", "-t", "c", "--sirt", "3", "--gpu", "--checkpoint", "s.mrc")
+    assert r.returncode == 2 and "need SIRT iterations" in r.stderr
