@@ -148,8 +148,8 @@ def barrier(dist, world):
 
 
 def hbm_peak():
-    """Measured HBM copy bandwidth of this pool's B200s (GB/s) and where it came from."""
-    for path in (os.path.join(ROOT, "MEASURED_PEAKS.json"), "/root/repo/MEASURED_PEAKS.json"):
+    """Measured HBM copy bandwidth of the B200s (GB/s) and where it came from."""
+    for path in (os.path.join(ROOT, "MEASURED_PEAKS.json"),):
         try:
             with open(path) as f:
                 v = json.load(f).get("hbm_gbs")
@@ -363,7 +363,7 @@ def run_ours(args):
                     "max_abs": float(np.abs(d).max()), "ref_max_abs": float(np.abs(ref).max()),
                     "slices": acc_rows}
     if rank == 0 and world == 1 and args.workload == "c2" and not args.no_serving:
-        # the metric's latency half and the north-star comparison: served FP16 against
+        # the metric's latency half and the target comparison: served FP16 against
         # serial plain FP32, end to end (host copies included), on the same series
         del proj_d
         torch.cuda.empty_cache()

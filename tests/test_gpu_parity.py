@@ -1,6 +1,6 @@
 """GPU parity: the CUDA path through the C ABI against the CPU oracle.
 
-Tolerances (the FP32 one is the north-star bound for the FP32 path):
+Tolerances (the FP32 one is the bound set for the FP32 path):
   * back-projection alone (no R-weighting, no stretch), FP32 storage: bit-exact
     against ref32 -- sample positions, fill rules, interpolation and the
     per-view accumulation order all follow the reference's f32 operations;
