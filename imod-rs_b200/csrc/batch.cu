@@ -9,6 +9,7 @@
 // batch, so each series' volume is bit-identical to its stand-alone result.
 #include <algorithm>
 #include <map>
+#include <tuple>
 #include <vector>
 
 #include "session_impl.h"
@@ -17,15 +18,17 @@ using namespace tg;
 
 namespace tg {
 
-// One persistent launch per (storage, z-factor) group of fast-path series;
-// other series get their own launch.  ntiles[i] receives the partial-stat
+// One persistent launch per (storage, z-factor, tile variant) group of fast-path
+// series, each series keeping the tile shape tuned for it; other series get
+// their own launch.  ntiles[i] receives the partial-stat
 // tile count written for ss[i] (used when modes[i] == 0).
 int batch_bp(tg_batch *b, const std::vector<tg_session *> &ss, const std::vector<int> &modes,
              std::vector<int> &ntiles, int *launches) {
   ntiles.assign(ss.size(), 0);
-  std::map<std::pair<int, int>, std::vector<int>> groups;
+  std::map<std::tuple<int, int, int>, std::vector<int>> groups;
   for (size_t i = 0; i < ss.size(); ++i) {
-    if (ss[i]->fast) groups[{ss[i]->store, ss[i]->zf_any ? 1 : 0}].push_back((int)i);
+    if (ss[i]->fast)
+      groups[std::make_tuple(ss[i]->store, ss[i]->zf_any ? 1 : 0, std::max(0, ss[i]->variant))].push_back((int)i);
     else {
       int rc = launch_bp(ss[i], modes[i], &ntiles[i]);
       if (rc != TG_OK) return rc;
@@ -34,9 +37,9 @@ int batch_bp(tg_batch *b, const std::vector<tg_session *> &ss, const std::vector
   }
   for (auto &kv : groups) {
     std::vector<int> &idx = kv.second;
-    // longest series (most views) first; its tuned tile shape serves the group
+    // longest series (most views) first in the tile queue
     std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return ss[x]->nviews > ss[y]->nviews; });
-    const int variant = std::max(0, ss[idx[0]]->variant);
+    const int variant = std::get<2>(kv.first);
     int S, TX, TZ;
     bp_fast_tile_shape(variant, &S, &TX, &TZ);
     std::vector<BpArgs> jobs;
@@ -68,7 +71,7 @@ int batch_bp(tg_batch *b, const std::vector<tg_session *> &ss, const std::vector
     bl.ntiles = (int)total;
     bl.counter = b->d_counter;
     bl.max_views = max_views;
-    int rc = launch_bp_batch(bl, kv.first.first, kv.first.second != 0, variant, b->st);
+    int rc = launch_bp_batch(bl, std::get<0>(kv.first), std::get<1>(kv.first) != 0, variant, b->st);
     if (rc != TG_OK) return rc;
     TG_CUDA(cudaGetLastError());
     ++*launches;

@@ -8,8 +8,8 @@
 //     same form share one launch per phase over a block table);
 //   * residual filter: series with the same register-resident FFT width,
 //     staging format and precision share one launch;
-//   * back-projection: one persistent launch per (precision, z-factor) group
-//     with a longest-first tile queue, as in batch_bp;
+//   * back-projection: one persistent launch per (precision, z-factor, tile
+//     variant) group with a longest-first tile queue, as in batch_bp;
 // series that fit no group (local alignment, general kernels, other widths)
 // get their own launches inside the same plan.  Each group kernel runs the
 // per-series body on each block's own series, so every series' result is the
@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <map>
+#include <tuple>
 #include <vector>
 
 #include "session_impl.h"
@@ -130,18 +131,18 @@ int round_plan_build(RoundPlan &p, const std::vector<tg_session *> &ss, const st
     p.fi.push_back(g);
   }
   // back-projection groups (batch_bp's grouping, SIRT update mode)
-  std::map<std::pair<int, int>, std::vector<tg_session *>> bpg;
+  std::map<std::tuple<int, int, int>, std::vector<tg_session *>> bpg;
   for (tg_session *s : ss) {
-    if (s->fast) bpg[{s->store, s->zf_any ? 1 : 0}].push_back(s);
+    if (s->fast) bpg[std::make_tuple(s->store, s->zf_any ? 1 : 0, std::max(0, s->variant))].push_back(s);
     else p.bp_single.push_back(s);
   }
   for (auto &kv : bpg) {
     std::vector<tg_session *> &mem = kv.second;
     std::stable_sort(mem.begin(), mem.end(), [](tg_session *x, tg_session *y) { return x->nviews > y->nviews; });
     RoundPlan::Bp g{};
-    g.store = kv.first.first;
-    g.zf = kv.first.second;
-    g.variant = std::max(0, mem[0]->variant);
+    g.store = std::get<0>(kv.first);
+    g.zf = std::get<1>(kv.first);
+    g.variant = std::get<2>(kv.first);
     int S, TX, TZ;
     bp_fast_tile_shape(g.variant, &S, &TX, &TZ);
     std::vector<BpArgs> jobs;
