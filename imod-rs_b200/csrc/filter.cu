@@ -414,13 +414,13 @@ __global__ void __launch_bounds__(256) filter_kernel(FilterArgs a) {
 
 // ---------------------------------------------------------------------------
 // Rows of 2^k (256..4096) or 3*2^k (384..3072) samples: register-resident
-// Stockham FFT.  N/V threads per row pair, each holding V complex values (8 for
-// 2^k: radix-8 passes, a transform of 2^L points in ceil(L/3) passes; 12 or 24
-// for 3*2^k: radix 8/4/2 passes and a final radix-3 pass), one shared-memory
-// exchange per pass (the generic kernel above takes one pass per factor 4).  The first forward pass
-// reads the rows from global memory, the weights are applied while the inverse
-// transform's first pass loads, and the epilogue works on the complex pairs
-// (row 2j in .x, row 2j+1 in .y) without splitting them.
+// Stockham FFT.  N/V threads per row pair, each holding V complex values (16 for
+// 1024..4096: radix-16 passes and a last radix 4, 8 or 16; 8 for 256 and 512:
+// radix-8 passes; 12 or 24 for 3*2^k: radix 8/4/2 passes and a final radix-3
+// pass), one shared-memory exchange per pass (the generic kernel above takes one
+// pass per factor 4).  The first forward pass reads the rows from global memory,
+// the spectrum stays in registers between the transforms, and the epilogue works
+// on the complex pairs (row 2j in .x, row 2j+1 in .y) without splitting them.
 // ---------------------------------------------------------------------------
 // Radix-4 butterfly with the plain complex sums and differences on the packed
 // f32x2 pipe (one instruction per complex add); the ones that meet a rotation by
@@ -469,8 +469,46 @@ template <bool INV> __device__ __forceinline__ void dft8(float2 *v) {
   }
 }
 
+// 16-point DFT as 4 x 4: radix-4 butterflies over v[j + 4m] (m), the twiddles
+// exp(-+2 pi i j k1 / 16), radix-4 butterflies over j; output in natural order.
+template <bool INV> __device__ __forceinline__ void dft16(float2 *v) {
+  // cos and sin of 2 pi m / 16 for the twiddle exponents m = j*k1 that occur
+  constexpr float c1 = 0.923879532511286756128183189396788933f;  // cos(pi/8)
+  constexpr float s1 = 0.382683432365089771728459984030398867f;  // sin(pi/8)
+  constexpr float h = 0.707106781186547524400844362104849039f;   // cos(pi/4)
+  float2 y[4][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    float2 q[4] = {v[j], v[j + 4], v[j + 8], v[j + 12]};
+    bfly4_p<INV, false>(q);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) y[j][k] = q[k];
+  }
+  auto tw = [](float2 z, float c, float sn) {  // z * (c - +i sn): the forward root exp(-i a)
+    const float2 w = make_float2(c, INV ? sn : -sn);
+    return cmul(z, w);
+  };
+  y[1][1] = tw(y[1][1], c1, s1);   // m = 1
+  y[1][2] = tw(y[1][2], h, h);     // m = 2
+  y[1][3] = tw(y[1][3], s1, c1);   // m = 3
+  y[2][1] = tw(y[2][1], h, h);     // m = 2
+  y[2][2] = rot<INV>(y[2][2]);     // m = 4: -+i
+  y[2][3] = tw(y[2][3], -h, h);    // m = 6
+  y[3][1] = tw(y[3][1], s1, c1);   // m = 3
+  y[3][2] = tw(y[3][2], -h, h);    // m = 6
+  y[3][3] = tw(y[3][3], -c1, -s1); // m = 9
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    float2 q[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+    bfly4_p<INV, false>(q);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = q[k2];
+  }
+}
+
 template <int R, bool INV> __device__ __forceinline__ void dft_r(float2 *v) {
-  if constexpr (R == 8) dft8<INV>(v);
+  if constexpr (R == 16) dft16<INV>(v);
+  else if constexpr (R == 8) dft8<INV>(v);
   else if constexpr (R == 4) bfly4_p<INV, false>(v);
   else if constexpr (R == 2) {
     const float2 a = v[0], b = v[1];
@@ -495,14 +533,15 @@ __device__ __forceinline__ int swz(int e) { return e + (e >> 4); }
 __device__ __forceinline__ int swz_add(int swz_e, int off) { return swz_e + off + (off >> 4); }
 template <int N> __host__ __device__ constexpr int padded_len() { return N + N / 16; }
 
-// Radix of pass i of the forward transform, for V values per thread: 8, 4 or 2
+// Radix of pass i of the forward transform, for V values per thread: 16, 8, 4 or 2
 // while the remaining length allows it (and V is a multiple), the factor 3 of
 // 3*2^k lengths last.
 __host__ __device__ constexpr int p2_radix(int N, int V, int i) {
   int NS = 1, R = 1;
   for (int p = 0; p <= i; ++p) {
     const int Q = N / NS;
-    R = (Q % 8 == 0 && V % 8 == 0) ? 8 : (Q % 4 == 0 && V % 4 == 0) ? 4 : (Q % 2 == 0 && V % 2 == 0) ? 2 : 3;
+    R = (Q % 16 == 0 && V % 16 == 0) ? 16 : (Q % 8 == 0 && V % 8 == 0) ? 8 : (Q % 4 == 0 && V % 4 == 0) ? 4
+        : (Q % 2 == 0 && V % 2 == 0) ? 2 : 3;
     NS *= R;
   }
   return R;
@@ -571,7 +610,8 @@ template <int LAY> __device__ __forceinline__ int p2_soff(int off) {
 // values per thread of the register-resident kernel for rows of n samples (0: none)
 static int p2_values(int n) {
   switch (n) {
-    case 256: case 512: case 1024: case 2048: case 4096: return 8;
+    case 256: case 512: return 8;
+    case 1024: case 2048: case 4096: return 16;
     case 384: return 12;
     case 768: case 1536: case 3072: return 24;
     default: return 0;
@@ -842,9 +882,14 @@ __device__ __forceinline__ void filter_p2_body(const FilterArgs &a, const int jp
   range_report<STORE>(a, hmax);
 }
 
-// at least 4 CTAs of 256 threads per SM (64 registers): the kernel is latency-bound
+// resident CTAs per SM the register allocation aims at (the kernel is latency-bound):
+// 4 of 256 threads for the radix-8 kernels; 5 of the radix-16 kernels' 64 or 128
+// threads (96 registers, no spills at 2048), 2 of 256
+__host__ __device__ constexpr int p2_min_blocks(int N, int V) {
+  return V == 8 && N / V == 256 ? 4 : V == 16 ? (N / V == 256 ? 2 : 5) : 1;
+}
 template <int N, int V, int FMT, int STORE>
-__global__ void __launch_bounds__(N / V, N / V == 256 ? 4 : 1) filter_p2_kernel(FilterArgs a) {
+__global__ void __launch_bounds__(N / V, p2_min_blocks(N, V)) filter_p2_kernel(FilterArgs a) {
   filter_p2_body<N, V, FMT, STORE>(a, blockIdx.x, blockIdx.y);
 }
 
@@ -852,7 +897,7 @@ __global__ void __launch_bounds__(N / V, N / V == 256 ? 4 : 1) filter_p2_kernel(
 // belongs to series j with blk0[j] <= b < blk0[j+1] ((ny+1)/2 row pairs x views
 // each); every series' rows come out as in its own launch.
 template <int N, int V, int FMT, int STORE>
-__global__ void __launch_bounds__(N / V, N / V == 256 ? 4 : 1) filter_p2_batch_kernel(FilterBatchDev fb) {
+__global__ void __launch_bounds__(N / V, p2_min_blocks(N, V)) filter_p2_batch_kernel(FilterBatchDev fb) {
   __shared__ __align__(16) FilterArgs s_a;
   __shared__ int s_j;
   if (threadIdx.x == 0) {
@@ -886,9 +931,9 @@ template <int FMT, int STORE> static bool try_p2(const FilterArgs &a, cudaStream
   switch (a.nx) {
     case 256: launch_p2<256, 8, FMT, STORE>(a, st); return true;
     case 512: launch_p2<512, 8, FMT, STORE>(a, st); return true;
-    case 1024: launch_p2<1024, 8, FMT, STORE>(a, st); return true;
-    case 2048: launch_p2<2048, 8, FMT, STORE>(a, st); return true;
-    case 4096: launch_p2<4096, 8, FMT, STORE>(a, st); return true;
+    case 1024: launch_p2<1024, 16, FMT, STORE>(a, st); return true;
+    case 2048: launch_p2<2048, 16, FMT, STORE>(a, st); return true;
+    case 4096: launch_p2<4096, 16, FMT, STORE>(a, st); return true;
     case 384: launch_p2<384, 12, FMT, STORE>(a, st); return true;  // 3 * 2^k: 12 or 24 values per thread
     case 768: launch_p2<768, 24, FMT, STORE>(a, st); return true;
     case 1536: launch_p2<1536, 24, FMT, STORE>(a, st); return true;
@@ -925,9 +970,9 @@ template <int FMT, int STORE> static void launch_batch_n(int n, const FilterBatc
   switch (n) {
     case 256: launch_p2_batch<256, 8, FMT, STORE>(fb, nb, st); break;
     case 512: launch_p2_batch<512, 8, FMT, STORE>(fb, nb, st); break;
-    case 1024: launch_p2_batch<1024, 8, FMT, STORE>(fb, nb, st); break;
-    case 2048: launch_p2_batch<2048, 8, FMT, STORE>(fb, nb, st); break;
-    case 4096: launch_p2_batch<4096, 8, FMT, STORE>(fb, nb, st); break;
+    case 1024: launch_p2_batch<1024, 16, FMT, STORE>(fb, nb, st); break;
+    case 2048: launch_p2_batch<2048, 16, FMT, STORE>(fb, nb, st); break;
+    case 4096: launch_p2_batch<4096, 16, FMT, STORE>(fb, nb, st); break;
     case 384: launch_p2_batch<384, 12, FMT, STORE>(fb, nb, st); break;
     case 768: launch_p2_batch<768, 24, FMT, STORE>(fb, nb, st); break;
     case 1536: launch_p2_batch<1536, 24, FMT, STORE>(fb, nb, st); break;
