@@ -1,7 +1,7 @@
 """Extract the boundary test vectors of the reference's own unit tests.
 
-Reads crates/imod-mrc/src/tests.rs and crates/imod-transforms/src/tests.rs of
-the imod-rs source tree (its root is given as argv[1], or in the environment
+Reads crates/imod-mrc/src/tests.rs, crates/imod-transforms/src/tests.rs and
+crates/imod-math/src/tests.rs of the imod-rs source tree (its root is given as argv[1], or in the environment
 variable IMOD_RS_SRC) and
 writes tests/golden/reference_vectors.json: for each reference test the
 constructor arguments, labels, statistics and the data-generating expression,
@@ -106,6 +106,19 @@ def main():
     src = open(os.path.join(SRC, "crates/imod-transforms/src/tilt.rs")).read()
     assert '"{:10.2}"' in src
     out["tilt_file_format"] = {"src": "crates/imod-transforms/src/tilt.rs:31", "format": "{:10.2}"}
+
+    # min_max_mean (crates/imod-math/src/stats.rs:844-861): the per-view mean fill and
+    # the output header statistics of the tilt path
+    mth = open(os.path.join(SRC, "crates/imod-math/src/tests.rs")).read()
+    b, ln = body(mth, "test_min_max_mean")
+    data = [float(x) for x in one(r"min_max_mean\(&\[([^\]]*)\]\)", b).split(",")]
+    out["min_max_mean"] = {
+        "src": f"crates/imod-math/src/tests.rs:{ln}", "data": data,
+        "min": one(r"assert_eq!\(min,\s*(-?[\d.]+)\)", b, float),
+        "max": one(r"assert_eq!\(max,\s*(-?[\d.]+)\)", b, float),
+        "mean_num": one(r"mean\s*-\s*([\d.]+)\s*/", b, float),
+        "mean_den": one(r"/\s*([\d.]+)\)\.abs\(\)", b, float),
+        "tol": one(r"abs\(\)\s*<\s*([\de.-]+)\)", b, float)}
 
     with open(OUT, "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)

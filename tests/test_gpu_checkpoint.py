@@ -109,3 +109,26 @@ def test_out_of_order_calls_are_refused():
         s.upload(proj)
         with pytest.raises(T.TiltGpuError):
             s.sirt_begin()
+
+
+def test_output_stage_and_view_mean_match_the_reference_unit_test():
+    # crates/imod-math/src/tests.rs test_min_max_mean (vector in tests/golden), through the
+    # device: the per-view mean of the uploaded view (tg_session_view_sums) and the output
+    # stage's header statistics of a volume restored into a SIRT run (tg_sirt_restore, then
+    # tg_sirt_end runs transform + statistics on it)
+    import json
+    import os
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_vectors.json")))["min_max_mean"]
+    data = np.array(g["data"], np.float32)
+    mean = g["mean_num"] / g["mean_den"]
+    nx = data.size
+    with T.Session(nx, 1, 1, np.zeros(1, np.float32), thickness=1, sirt=1) as s:
+        s.upload(data.reshape(1, 1, nx))
+        assert abs(s.view_sums()[0] / nx - mean) < g["tol"]
+        assert s.out_shape == (1, 1, nx)
+        s.sirt_restore(data.reshape(1, 1, nx), 1)  # all iterations done: output stage only
+        s.sirt_end()
+        vol, st = s.download()
+    np.testing.assert_array_equal(vol.reshape(-1), data)  # densweight 1, outscale 1, outadd 0
+    assert st["amin"] == g["min"] and st["amax"] == g["max"]
+    assert abs(st["amean"] - mean) < g["tol"]

@@ -226,3 +226,18 @@ def test_studio_step_is_tilt_with_its_options():
     tilt2, _ = O.run(O.Params(nx, ny, nz, ang[:7], thickness=nx, no_weight=True, no_cosine_stretch=True,
                               fill_mode="zero"), proj, 32)
     np.testing.assert_array_equal(studio2, tilt2)
+
+
+def test_min_max_mean_matches_the_reference_unit_test():
+    # crates/imod-math/src/tests.rs test_min_max_mean (vector in tests/golden): the per-view
+    # mean fill (main.rs:616-623) and the output header statistics (main.rs:1077-1093)
+    import json
+    import os
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_vectors.json")))["min_max_mean"]
+    data = np.array(g["data"], np.float32)
+    mean = g["mean_num"] / g["mean_den"]
+    m = O.view_means(data.reshape(1, 1, -1))
+    assert abs(float(m[0]) - mean) < g["tol"]
+    _, st = O.output_stats(data.reshape(1, 1, -1))
+    assert st["amin"] == g["min"] and st["amax"] == g["max"]
+    assert abs(st["amean"] - mean) < g["tol"]
