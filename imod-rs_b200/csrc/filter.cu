@@ -552,16 +552,16 @@ __host__ __device__ constexpr int p2_npass(int N, int V) {
   return p;
 }
 // span (product of the earlier passes' radices) of pass i
-__host__ __device__ constexpr int p2_span(int N, int V, bool inv, int i) {
+__host__ __device__ constexpr int p2_span(int N, int V, int i) {
   int NS = 1;
-  for (int p = 0; p < i; ++p) NS *= p2_radix(N, V, inv ? p2_npass(N, V) - 1 - p : p);
+  for (int p = 0; p < i; ++p) NS *= p2_radix(N, V, p);
   return NS;
 }
 // offset of forward pass i's twiddles in the per-pass table: (R-1)*NS entries
 // per earlier pass with twiddles (NS > 1; n - R0 entries in all, R0 the first radix)
 __host__ __device__ constexpr int p2_twoff(int N, int V, int i) {
   int off = 0;
-  for (int p = 1; p < i; ++p) off += (p2_radix(N, V, p) - 1) * p2_span(N, V, false, p);
+  for (int p = 1; p < i; ++p) off += (p2_radix(N, V, p) - 1) * p2_span(N, V, p);
   return off;
 }
 // Shared-memory layout of the buffer a pass writes.  LAY_PAD (swz): one slot of
@@ -574,7 +574,7 @@ __host__ __device__ constexpr int p2_twoff(int N, int V, int i) {
 // bank pairs, so the lane-contiguous accesses stay conflict-free.
 enum { LAY_PAD = 0, LAY_XOR8 = 1, LAY_LIN = 2 };
 __host__ __device__ constexpr int p2_layout(int N, int V, int p) {
-  return (p2_radix(N, V, p) == 8 && p2_span(N, V, false, p) == 8) ? LAY_XOR8 : LAY_PAD;
+  return (p2_radix(N, V, p) == 8 && p2_span(N, V, p) == 8) ? LAY_XOR8 : LAY_PAD;
 }
 // slot of element t + j*T (lane-contiguous accesses)
 template <int LAY, int T> __device__ __forceinline__ int p2_cslot(int t, int j) {
@@ -624,7 +624,7 @@ bool p2_twiddle_table(int n, std::vector<float2> &out) {
   if (!V) return false;
   out.resize((size_t)n - p2_radix(n, V, 0));
   for (int p = 0; p < p2_npass(n, V); ++p) {
-    const int R = p2_radix(n, V, p), NS = p2_span(n, V, false, p), off = p2_twoff(n, V, p);
+    const int R = p2_radix(n, V, p), NS = p2_span(n, V, p), off = p2_twoff(n, V, p);
     if (NS == 1) continue;
     for (int r = 1; r < R; ++r)
       for (int k = 0; k < NS; ++k) {
@@ -644,7 +644,7 @@ template <int N, int V, int I, bool TOREG>
 __device__ __forceinline__ void p2_pass(float2 (&x)[V], int t, const float2 *__restrict__ tw, float2 *Y) {
   constexpr int T = N / V;
   constexpr int R = p2_radix(N, V, I);
-  constexpr int NS = p2_span(N, V, false, I);
+  constexpr int NS = p2_span(N, V, I);
   constexpr int M = V / R;  // butterflies per thread
   static_assert(V % R == 0, "values per thread must be a multiple of the radix");
   static_assert(!TOREG || NS * R == N, "only the last pass keeps its results in registers");
@@ -707,7 +707,7 @@ __device__ __forceinline__ void p2_ipass(float2 (&x)[V], int t, const float2 *__
   constexpr int T = N / V;
   constexpr int PF = p2_npass(N, V) - 1 - I;
   constexpr int R = p2_radix(N, V, PF);
-  constexpr int NS = p2_span(N, V, false, PF);
+  constexpr int NS = p2_span(N, V, PF);
   constexpr int M = V / R;
   static_assert(I == 0 || ((NS & (NS - 1)) == 0 && R != 3), "folded offsets need power-of-two spans and radices");
 #pragma unroll
