@@ -176,6 +176,7 @@ __device__ __forceinline__ void fp_fast_body(const FpArgs &a, const int bx, cons
     while (lo < a.onx && x < lo_t) { ++lo; flo += 1.0f; x = X(flo, t2); }
     const float *vz = a.vol + (size_t)oz * a.onx;
     float fo = flo;
+#pragma unroll 2
     for (int ox = lo; ox < a.onx; ++ox, fo += 1.0f, x = X(fo, t2)) {
       if (!(x < hi_t)) break;
       const float tt = __fadd_rd(x, FMAGIC);
@@ -432,6 +433,7 @@ __device__ __forceinline__ void fp_half_body(const FpArgs &a, const int bx, cons
     while (lo < a.onx && x < lo_t) { ++lo; flo += 1.0f; x = X(flo); }
     const uint4 *vz = vg + (size_t)oz * a.onx * (S / 8);
     float fo = flo;
+#pragma unroll 2
     for (int ox = lo; ox < a.onx; ++ox, fo += 1.0f, x = X(fo)) {
       if (!(x < hi_t)) break;
       const float tt = __fadd_rd(x, FMAGIC);
