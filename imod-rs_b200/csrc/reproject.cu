@@ -419,8 +419,6 @@ __device__ __forceinline__ void fp_half_body(const FpArgs &a, const int bx, cons
   const float c = XT ? cos_t * cos_xt : cos_t;
   float c0 = 0.0f;
   auto X = [&](float fo) { return fmaf(fo, c, c0); };  // fo: the column as a float
-  const float pf = (float)p;
-  const bool ok_hi = p <= a.nx - 2, ok_lo = p >= 1;  // floor p needs bin p+1, floor p-1 needs bin p-1
   const uint4 *vg = reinterpret_cast<const uint4 *>(a.volh) + (size_t)bz * a.onz * a.onx * (S / 8);
   float foz = 0.0f;
   for (int oz = 0; oz < a.onz; ++oz, foz += 1.0f) {
@@ -438,12 +436,11 @@ __device__ __forceinline__ void fp_half_body(const FpArgs &a, const int bx, cons
 #pragma unroll 2
     for (int ox = lo; ox < a.onx; ++ox, fo += 1.0f, x = X(fo)) {
       if (!(x < hi_t)) break;
-      // x in [p-1, p+1): the weight of bin p is 1 - |x - p| (1 - f for floor p, f for
-      // floor p-1); the reference's bounds rule (both bins of the floor in range) drops
-      // only the edge bins' outer halves
-      const float d = x - pf;
-      if (d >= 0.0f ? !ok_hi : !ok_lo) continue;
-      const __half2 w2 = __float2half2_rn(1.0f - fabsf(d));
+      const float tt = __fadd_rd(x, FMAGIC);
+      const int x0 = (int)(__float_as_uint(tt) - FMAGIC_BITS);
+      if ((unsigned)x0 > (unsigned)(a.nx - 2)) continue;
+      const float frac = __fsub_rn(x, __fsub_rn(tt, FMAGIC));
+      const __half2 w2 = __float2half2_rn(x0 == p ? __fsub_rn(1.0f, frac) : frac);
       const uint4 *q = vz + ox;  // plane k of this column at q + k*onx
 #pragma unroll
       for (int k = 0; k < S / 8; ++k) {
