@@ -518,11 +518,12 @@ template <int R, bool INV> __device__ __forceinline__ void dft_r(float2 *v) {
 }
 
 // Shared-memory position of row element e: one padding slot after every 16
-// complex values (128 bytes, one pass over the 32 banks).  Unpadded, the radix-8
-// passes at spans 1 and 8 store with strides of 8 and 64 values, which put 16 and
-// 4 lanes of a warp on the same banks; padded, every bank pair takes exactly two
-// of a warp's 32 stores in every pass, and reads of consecutive elements stay
-// conflict-free.  A pass's R outputs sit at e + r*NS with the low four bits of e
+// complex values (128 bytes, one pass over the 32 banks).  Unpadded, a span-1
+// pass stores with a stride of R values (8 or 16), which puts the lanes of a
+// half-warp on a few bank pairs; padded, the half-warp's 16 stores land on 16
+// distinct bank pairs in the span-1 passes and at spans of 16 or more, and reads
+// of consecutive elements stay conflict-free (the radix-8 pass at span 8 writes
+// the LAY_XOR8 layout below instead).  A pass's R outputs sit at e + r*NS with the low four bits of e
 // and r*NS never carrying into bit 4, so their padded positions are one base plus
 // compile-time offsets (no per-element address arithmetic).
 __device__ __forceinline__ int swz(int e) { return e + (e >> 4); }
