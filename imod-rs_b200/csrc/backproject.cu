@@ -586,8 +586,6 @@ static const FastVariant kFast[] = {
     {8, 4, 64, 256, 4, 3, "S8K4TX64NT256V4N3"},
     {16, 2, 64, 256, 4, 3, "S16K2TX64NT256V4N3"},
     {16, 2, 32, 256, 4, 3, "S16K2TX32NT256V4N3"},
-    {8, 4, 64, 256, 8, 3, "S8K4TX64NT256V8N3"},
-    {8, 4, 64, 256, 8, 2, "S8K4TX64NT256V8N2"},
 };
 constexpr int MAX_S = 16;  // rows per tile of the widest variant (sizes the staging buffer)
 int bp_fast_variants() { return (int)(sizeof(kFast) / sizeof(kFast[0])); }
@@ -647,8 +645,6 @@ static int launch_fast_v(const BpArgs &a, int variant, cudaStream_t st, int *nti
     case 10: return launch_fast_t<STORE, 8, 4, 32, 256, 8, 3, ZF>(a, st, ntiles);
     case 12: return launch_fast_t<STORE, 16, 2, 64, 256, 4, 3, ZF>(a, st, ntiles);
     case 13: return launch_fast_t<STORE, 16, 2, 32, 256, 4, 3, ZF>(a, st, ntiles);
-    case 14: return launch_fast_t<STORE, 8, 4, 64, 256, 8, 3, ZF>(a, st, ntiles);
-    case 15: return launch_fast_t<STORE, 8, 4, 64, 256, 8, 2, ZF>(a, st, ntiles);
     default: return launch_fast_t<STORE, 8, 4, 64, 256, 4, 3, ZF>(a, st, ntiles);
   }
 }
@@ -669,8 +665,6 @@ static int launch_batch_v(const BatchLaunch &bl, int variant, cudaStream_t st) {
     case 10: return launch_batch_t<STORE, 8, 4, 32, 256, 8, 3, ZF>(bl, st);
     case 12: return launch_batch_t<STORE, 16, 2, 64, 256, 4, 3, ZF>(bl, st);
     case 13: return launch_batch_t<STORE, 16, 2, 32, 256, 4, 3, ZF>(bl, st);
-    case 14: return launch_batch_t<STORE, 8, 4, 64, 256, 8, 3, ZF>(bl, st);
-    case 15: return launch_batch_t<STORE, 8, 4, 64, 256, 8, 2, ZF>(bl, st);
     default: return launch_batch_t<STORE, 8, 4, 64, 256, 4, 3, ZF>(bl, st);
   }
 }
