@@ -524,8 +524,15 @@ __global__ void __launch_bounds__(NT + 32) bp_fast_kernel(const __grid_constant_
 // tile of the queue (longest series first) until it is empty.  Each tile's
 // arithmetic is the same as in the per-series kernel, so every series' result
 // does not depend on what else is in the batch.
+// Resident CTAs per SM: the per-series kernel's 32-accumulator shapes fit three
+// 288-thread (five 160-thread) CTAs in the register file; without a bound the
+// tile loop's extra state takes this kernel to 84-96 registers and two (four)
+// CTAs, a third less throughput.  The bound keeps the per-series occupancy.
+template <int S, int K, int NT> constexpr int batch_min_ctas() {
+  return S * K > 32 ? 1 : NT == 256 ? 3 : 5;
+}
 template <int STORE, int S, int K, int TX, int NT, int VPS, int NSTAGE, int ZF>
-__global__ void __launch_bounds__(NT + 32) bp_batch_kernel(const BpArgs *__restrict__ jobs, int njobs,
+__global__ void __launch_bounds__(NT + 32, (batch_min_ctas<S, K, NT>())) bp_batch_kernel(const BpArgs *__restrict__ jobs, int njobs,
                                                            int ntiles, int *counter, int max_views) {
   using C = FastCfg<STORE, S, K, TX, NT, VPS, NSTAGE, ZF>;
   extern __shared__ __align__(128) unsigned char sm[];
