@@ -417,6 +417,43 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
   const bool xok = oxr < a.onx;
   float *red = reinterpret_cast<float *>(sm);  // staging buffers are free now
   const int tile = bx + by * a.nbx;
+  auto acc_at = [&](int s, int j) {
+    if constexpr (STORE == TG_STORE_FP32) {
+      const float2 p = up2(acc2[s / 2][j]);
+      return (s & 1) ? p.y : p.x;
+    } else {
+      return acc[s < NACC ? s : 0][j];
+    }
+  };
+  if (a.mode == 2) {
+    // SIRT update vol += relax * v.  The old values of SG slices (8 values) are
+    // loaded together before any of their stores: a store through vol could
+    // alias a later load as far as the compiler knows, which would otherwise
+    // make each of the S*K updates wait for its own round trip to HBM.
+    constexpr int SG = 1;
+    const int ozt = oz0 + tzg, zstep = OZG * a.onx;  // depth j of a slice: + j * zstep
+#pragma unroll
+    for (int s0 = 0; s0 < S; s0 += SG) {
+      float old[SG][K];
+      float *rows[SG];
+#pragma unroll
+      for (int g = 0; g < SG; ++g) {
+        rows[g] = a.vol + ((size_t)(iy0 + s0 + g) * a.onz + ozt) * a.onx + oxr;
+        const bool yok = xok && iy0 + s0 + g < a.ny;
+#pragma unroll
+        for (int j = 0; j < K; ++j) old[g][j] = (yok && ozt + j * OZG < a.onz) ? rows[g][j * zstep] : 0.0f;
+      }
+#pragma unroll
+      for (int g = 0; g < SG; ++g) {
+        const bool yok = xok && iy0 + s0 + g < a.ny;
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+          if (yok && ozt + j * OZG < a.onz)
+            rows[g][j * zstep] = __fadd_rn(old[g][j], __fmul_rn(a.relax, __fmul_rn(acc_at(s0 + g, j), a.inv_n)));
+      }
+    }
+    return true;
+  }
 #pragma unroll
   for (int s = 0; s < S; ++s) {
     const int iy = iy0 + s;
@@ -427,24 +464,15 @@ __device__ __forceinline__ bool bp_tile(const BpArgs &a, int bx, int by, int bz,
       const int oz = oz0 + tzg + j * OZG;
       if (xok && oz < a.onz && iy < a.ny) {
         const size_t idx = ((size_t)iy * a.onz + oz) * a.onx + oxr;
-        float accv;
-        if constexpr (STORE == TG_STORE_FP32) {
-          const float2 p = up2(acc2[s / 2][j]);
-          accv = (s & 1) ? p.y : p.x;
-        } else {
-          accv = acc[s < NACC ? s : 0][j];
-        }
-        const float v = __fmul_rn(accv, a.inv_n);
+        const float v = __fmul_rn(acc_at(s, j), a.inv_n);
         if (a.mode == 0) {
           const float y = __fadd_rn(__fmul_rn(__fmul_rn(v, a.dw), a.os), a.oa);
           a.vol[idx] = y;
           mn = fminf(mn, y);
           mx = fmaxf(mx, y);
           sum += (double)y;
-        } else if (a.mode == 1) {
+        } else {  // mode 1
           a.vol[idx] = v;
-        } else {
-          a.vol[idx] = __fadd_rn(a.vol[idx], __fmul_rn(a.relax, v));
         }
       }
     }
