@@ -831,6 +831,21 @@ __global__ void __launch_bounds__(NT) bp_general_kernel(BpArgs a) {
   }
   // epilogue (same as the fast kernel)
   const bool xok = ox < a.onx;
+  if (a.mode == 2) {  // vol += relax * v: the K old values are loaded before any store
+    float old[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      const int oz = oz0 + tzg + j * OZG;
+      old[j] = (xok && oz < a.onz) ? a.vol[((size_t)iy * a.onz + oz) * a.onx + ox] : 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      const int oz = oz0 + tzg + j * OZG;
+      if (xok && oz < a.onz)
+        a.vol[((size_t)iy * a.onz + oz) * a.onx + ox] = __fadd_rn(old[j], __fmul_rn(a.relax, __fmul_rn(acc[j], a.inv_n)));
+    }
+    return;
+  }
   float mn = 3.40282347e+38f, mx = -3.40282347e+38f;
   double sum = 0.0;
 #pragma unroll
@@ -845,10 +860,8 @@ __global__ void __launch_bounds__(NT) bp_general_kernel(BpArgs a) {
         mn = fminf(mn, y);
         mx = fmaxf(mx, y);
         sum += (double)y;
-      } else if (a.mode == 1) {
+      } else {  // mode 1
         a.vol[idx] = v;
-      } else {
-        a.vol[idx] = __fadd_rn(a.vol[idx], __fmul_rn(a.relax, v));
       }
     }
   }

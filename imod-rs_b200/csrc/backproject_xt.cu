@@ -246,6 +246,13 @@ __global__ void __launch_bounds__(XT_TX * XT_NW, 5) bp_xtilt_kernel(BpArgs a) {
     float mn = 3.40282347e+38f, mx = -3.40282347e+38f;
     double sum = 0.0;
     if (iy < a.ny) {
+      // SIRT update: the slice's K old values are loaded before any of its stores
+      float old[K];
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        const int oz = oz0 + wz + j * XT_NW;
+        old[j] = (a.mode == 2 && xok && oz < a.onz) ? a.vol[((size_t)iy * a.onz + oz) * a.onx + ox] : 0.0f;
+      }
 #pragma unroll
       for (int j = 0; j < K; ++j) {
         const int oz = oz0 + wz + j * XT_NW;
@@ -261,7 +268,7 @@ __global__ void __launch_bounds__(XT_TX * XT_NW, 5) bp_xtilt_kernel(BpArgs a) {
           } else if (a.mode == 1) {
             a.vol[idx] = vv;
           } else {
-            a.vol[idx] = __fadd_rn(a.vol[idx], __fmul_rn(a.relax, vv));
+            a.vol[idx] = __fadd_rn(old[j], __fmul_rn(a.relax, vv));
           }
         }
       }
@@ -325,22 +332,46 @@ __global__ void __launch_bounds__(256) xt_blend_kernel(BpArgs a, const float *__
     const float w0 = __fsub_rn(1.0f, fr);
     const float *b0 = rows + ((two || one) ? (size_t)sy0 * sl : 0) + ox;
     float *out = a.vol + (size_t)iy * sl + ox;
-#pragma unroll 4
-    for (int oz = oz0; oz < oz1; ++oz) {
-      const size_t o = (size_t)oz * a.onx;
+    auto blend = [&](size_t o) {
       float v = 0.0f;
       if (two) v = __fadd_rn(__fmul_rn(__ldg(b0 + o), w0), __fmul_rn(__ldg(b0 + sl + o), fr));
       else if (one) v = __ldg(b0 + o);
+      return v;
+    };
+    if (MODE == 2) {
+      // vol += relax * v, four depths at a time: their old values are loaded
+      // before any of their stores (a store through out could alias a later
+      // load as far as the compiler knows, so one update at a time would wait
+      // for each load's round trip to HBM in turn)
+      int oz = oz0;
+      for (; oz + 4 <= oz1; oz += 4) {
+        float old[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) old[u] = out[(size_t)(oz + u) * a.onx];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const size_t o = (size_t)(oz + u) * a.onx;
+          out[o] = __fadd_rn(old[u], __fmul_rn(a.relax, blend(o)));
+        }
+      }
+      for (; oz < oz1; ++oz) {
+        const size_t o = (size_t)oz * a.onx;
+        out[o] = __fadd_rn(out[o], __fmul_rn(a.relax, blend(o)));
+      }
+      continue;
+    }
+#pragma unroll 4
+    for (int oz = oz0; oz < oz1; ++oz) {
+      const size_t o = (size_t)oz * a.onx;
+      const float v = blend(o);
       if (MODE == 0) {
         const float y = __fadd_rn(__fmul_rn(__fmul_rn(v, a.dw), a.os), a.oa);
         out[o] = y;
         mn = fminf(mn, y);
         mx = fmaxf(mx, y);
         sum += (double)y;
-      } else if (MODE == 1) {
+      } else {  // MODE 1
         out[o] = v;
-      } else {
-        out[o] = __fadd_rn(out[o], __fmul_rn(a.relax, v));
       }
     }
   }
