@@ -163,19 +163,21 @@ def hbm_peak():
 def read_traffic(variant_name, storage="fp16"):
     """Per-launch DRAM bytes of the back-projection kernel at the large configuration,
     from the committed ncu summary of that tile variant (a 256-row strip of the same
-    geometry, scaled by 2048 / 256 rows), or None when the timed variant has none."""
+    geometry, scaled by 2048 / 256 rows), or None when the timed variant has none.
+    The summary lists one or more captures, each a `variant:` line followed by its
+    `traffic_bytes_per_launch:` line."""
     path = os.path.join(ROOT, "profiles", f"bp_fast_c2strip_{storage}.md")
-    vals = {}
+    traffic, cur = {}, None
     try:
         for line in open(path):
-            if ":" in line and line.split(":", 1)[0] in ("variant", "traffic_bytes_per_launch"):
-                k, v = line.split(":", 1)
-                vals[k] = v.strip()
+            key, _, val = line.partition(":")
+            if key == "variant":
+                cur = val.strip()
+            elif key == "traffic_bytes_per_launch" and cur is not None:
+                traffic[cur] = float(val.strip())
     except OSError:
         return None
-    if vals.get("variant") != variant_name or "traffic_bytes_per_launch" not in vals:
-        return None
-    return float(vals["traffic_bytes_per_launch"])
+    return traffic.get(variant_name)
 
 
 def run_ours(args):
