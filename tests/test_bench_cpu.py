@@ -48,3 +48,23 @@ def test_hbm_peak_is_read_from_the_measured_file(tmp_path, monkeypatch):
     (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"hbm_gbs": 6463.0}))
     v, how = bench.hbm_peak()
     assert v == 6463.0 and "measured" in how
+
+
+def test_roofline_traffic_comes_from_the_capture_of_the_timed_tile_shape():
+    # the committed summaries list one capture per tile shape the tuner picks; each
+    # `variant:` line is followed by that capture's per-launch DRAM bytes
+    for storage in ("fp16", "fp32"):
+        seen = {}
+        cur = None
+        for line in open(os.path.join(ROOT, "profiles", f"bp_fast_c2strip_{storage}.md")):
+            key, _, val = line.partition(":")
+            if key == "variant":
+                cur = val.strip()
+            elif key == "traffic_bytes_per_launch":
+                seen.setdefault(cur, float(val))
+        assert set(seen) >= {"S8K4TX64NT256V4N3", "S8K4TX32NT256V8N2"}
+        for name, want in seen.items():
+            assert bench.read_traffic(name, storage) == want
+            # staged windows once + the 13.42 GB volume once (about 15.1 GB FP16, 17.2 GB FP32)
+            assert 13.4e9 < want < 18e9
+    assert bench.read_traffic("S16K2TX32NT256V4N3", "fp16") is None  # no capture: no claim
